@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""Throughput of the template-matching search on one node.
+
+One step = the full search of one synthetic micrograph (default: 4096^2, 200
+templates of 180^2, 72 in-plane angles, norm_type=1, 512 windows with 192 px
+overlap) with the inputs resident in device memory.  Every rank searches its own
+micrograph (micrographs are independent: replicas, no collective), so scaling is
+weak and `value` is the whole-job micrographs/s.  `e2e` repeats the measurement
+through gisspa_search with the micrograph in pinned host memory (host->device
+copy and the pick read-back inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form plain|fp16|topk|fp16_topk]
+
+`--impl reference` times the reference algorithm's CPU restatement (the FP64
+oracle; the reference itself has no CPU path) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "gisspa_v2.0_b200"))
+import gisspa  # noqa: E402
+import synth  # noqa: E402
+
+METRIC = "micrographs/s and template-rotations/s vs plain FP32 path at ≤1e-3 score err"
+
+FORMS = {
+    "plain": dict(spectrum_precision=gisspa.SPEC_FP32, pick_mode=gisspa.PICK_CHUNK),
+    "fp16": dict(spectrum_precision=gisspa.SPEC_FP16, pick_mode=gisspa.PICK_CHUNK),
+    "topk": dict(spectrum_precision=gisspa.SPEC_FP32, pick_mode=gisspa.PICK_TOPK),
+    "fp16_topk": dict(spectrum_precision=gisspa.SPEC_FP16, pick_mode=gisspa.PICK_TOPK),
+}
+
+
+def args_parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="whole_4096_t200", choices=list(synth.WORKLOADS))
+    ap.add_argument("--form", default="plain", choices=list(FORMS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of this rank's GPU during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ roofline
+def measured_peak_hbm():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(L: int, spec: int, D: float):
+    """Per (window, template-rotation) pair, split per kernel:
+    B = H b_t + 2 H b_m + (H b_i + L^2 b_s) / D, H = L (L/2 + 1)."""
+    H = L * (L // 2 + 1)
+    b_t = 8 if spec == gisspa.SPEC_FP32 else 4
+    b_m, b_i, b_s = 8, 8, 48
+    pass_a = H * b_t + H * b_m + H * b_i / D
+    pass_b = H * b_m + L * L * b_s / D
+    return pass_a, pass_b
+
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary, when present."""
+    p = os.path.join(REPO, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as fh:
+            return json.load(fh).get(kernel)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------ CPU leg (the FP64 oracle)
+def oracle_rate(case, cfg, n_angles: int):
+    """Micrograph time of the FP64 oracle on the host cores, from two bounded samples of the
+    same workload (1 and 3 templates at one angle): slope = cost of one template-rotation
+    over all windows (both sweeps), intercept = per-micrograph preparation."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+
+    ctf = gisspa.Ctf(case.defocus, case.dfdiff, case.dfang)
+    t = []
+    for nts in (1, 3):
+        t0 = time.perf_counter()
+        oracle.search(cfg, ctf, case.image, case.templates, max_templates=nts, max_angles=1)
+        t.append(time.perf_counter() - t0)
+    per_rot = max((t[1] - t[0]) / 2.0, 1e-9)
+    prep = max(t[0] - per_rot, 0.0)
+    nt = case.templates.shape[0]
+    mic_s = prep + per_rot * nt * n_angles
+    return 1.0 / mic_s, oracle.num_threads(), sum(t), per_rot, prep
+
+
+# ------------------------------------------------------------------ main
+def main():
+    a = args_parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    wl = a.workload
+    params = dict(synth.SEARCH_PARAMS[wl])
+    params.update(FORMS[a.form])
+    cfg = gisspa.Config.default(**params)
+    angles = int(math.ceil(360.0 / cfg.phistep - 1e-9))
+    data = dict(synth.WORKLOADS[wl])
+    config_desc = {"workload": wl, "form": a.form, "image": list(data["shape"]), "templates": data["n_templates"],
+                   "template_size": data["tsize"], "angles": angles, "window_size": cfg.window_size,
+                   "overlap": cfg.overlap, "norm_type": cfg.norm_type, "parallelism": f"replicas{world}",
+                   "l2": "working set > 1 GB per step (larger than L2)"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        case = synth.make_case(**data)
+        steps = []
+        for i in range(a.warmup + a.steps):
+            r = oracle_rate(case, cfg, angles)
+            if i >= a.warmup:
+                steps.append(r)
+        rate = float(np.mean([s[0] for s in steps]))
+        cores = steps[0][1]
+        sample = (f"FP64 oracle, {wl}: 1 and 3 templates x 1 angle over all windows (both sweeps), "
+                  f"extrapolated linearly to {data['n_templates']} templates x {angles} angles")
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": rate, "unit": "micrographs/s",
+                          "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
+                          "template_rotations_per_s": rate * data["n_templates"] * angles,
+                          "ms_per_step": 1000.0 / rate, "dtype": "f64", "data": "synthetic", "config": config_desc,
+                          "cpu_baseline": {"value": rate, "unit": "micrographs/s", "cores": cores, "kind": "port",
+                                           "sample": sample},
+                          "e2e": {"value": rate, "unit": "micrographs/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    case = synth.make_case(**{**data, "seed": data["seed"] + 1000 * rank})
+    s = gisspa.Searcher(cfg, local)
+    s.set_templates(case.templates)
+    ny, nx = case.image.shape
+    d_img = torch.from_numpy(case.image).to(dev)
+    out = np.zeros(1 << 22, dtype=gisspa.PICK_DTYPE)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(a.warmup):
+        s.search_device(d_img.data_ptr(), nx, ny, gisspa.Ctf(case.defocus, case.dfdiff, case.dfang), out)
+    torch.cuda.synchronize()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    smi_index = int(vis.split(",")[local]) if vis and vis.split(",")[local].strip().isdigit() else local
+    clocks = ClockSampler(smi_index)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    launches, npicks, stats = 0, 0, []
+    ctf = gisspa.Ctf(case.defocus, case.dfdiff, case.dfang)
+    for _ in range(a.steps):
+        npicks = s.search_device(d_img.data_ptr(), nx, ny, ctf, out)
+        st = s.stats()
+        launches += st.kernel_launches
+        stats.append(st)
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * a.steps / (ms_max / 1000.0)
+
+    e2e = None
+    if not a.no_e2e:
+        host = torch.from_numpy(case.image).pin_memory()
+        himg = host.numpy()
+        s.search(himg, ctf)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n_e2e = 0
+        for _ in range(a.steps):
+            picks = s.search(himg, ctf)
+            n_e2e = len(picks)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        te = torch.tensor([el], device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+        e2e = {"value": world * a.steps / float(te.item()), "unit": "micrographs/s",
+               "h2d_bytes_per_step": int(nx * ny * 4), "d2h_bytes_per_step": int(n_e2e * gisspa.PICK_DTYPE.itemsize),
+               "timing": "host wall clock around the synchronous C-ABI call, max over ranks"}
+
+    # roofline of the correlation kernels (sampled CUDA-event durations inside the timed steps)
+    st_a = np.mean([x.pass_a_us for x in stats])
+    st_b = np.mean([x.pass_b_us for x in stats])
+    ppl = np.mean([x.pairs_per_launch for x in stats])
+    dpl = np.mean([x.templates_per_launch for x in stats])
+    ba, bb = algorithmic_bytes(cfg.window_size, cfg.spectrum_precision, max(dpl, 1.0))
+    peak, peak_kind = measured_peak_hbm()
+    kern = "pass_b" if st_b >= st_a else "pass_a"
+    dur = st_b if kern == "pass_b" else st_a
+    alg = (bb if kern == "pass_b" else ba) * ppl
+    achieved = alg / (dur * 1e-6) / 1e9 if dur > 0 else 0.0
+    tr = traffic_from_profiles(kern)
+    roofline = {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind, "traffic": tr,
+                "bytes_per_launch": alg, "launch_us": dur, "pass_a_us": st_a, "pass_b_us": st_b,
+                "pairs_per_launch": ppl, "templates_per_launch": dpl}
+
+    res = None
+    if rank == 0:
+        res = {"metric": METRIC, "value": value, "unit": "micrographs/s", "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32" if cfg.spectrum_precision == 0 else "f16-spectra/f32",
+               "data": "synthetic (seeded Gaussian-blob projections planted in N(0,1) noise)",
+               "config": config_desc,
+               "template_rotations_per_s": value * data["n_templates"] * angles,
+               "pairs_per_step": int(stats[-1].pairs), "picks_per_step": int(npicks),
+               "stage_ms": {"prep": stats[-1].ms_prep, "sweep1": stats[-1].ms_sweep1,
+                            "sweep2": stats[-1].ms_sweep2, "pick": stats[-1].ms_pick},
+               "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "e2e": e2e}
+        if world == 1 and not a.no_cpu_baseline:
+            rate, cores, secs, per_rot, prep = oracle_rate(case, cfg, angles)
+            res["cpu_baseline"] = {"value": rate, "unit": "micrographs/s", "cores": cores, "kind": "port",
+                                   "sample": f"FP64 oracle, 1 and 3 templates x 1 angle over all windows "
+                                             f"({secs:.1f} s), extrapolated to the full workload"}
+        print(json.dumps(res))
+    s.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,108 @@
+// common.cuh — shared device/host helpers for the B200 search library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+
+namespace gisspa {
+
+// pi used where the reference uses its own PI constant (utils/constants.h:3)
+constexpr double kRefPi = 3.1415926535;
+constexpr double kPi = 3.14159265358979323846;
+
+struct CudaError {
+  cudaError_t code;
+  std::string where;
+};
+
+#define GISSPA_CUDA(call)                                                               \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      throw ::gisspa::CudaError{e_, std::string(#call) + " @ " + __FILE__ + ":" +       \
+                                        std::to_string(__LINE__)};                      \
+  } while (0)
+
+// Number of kernels this library has launched from the calling thread.
+long long& launch_counter();
+
+#define GISSPA_LAUNCH_CHECK()              \
+  do {                                     \
+    ++::gisspa::launch_counter();          \
+    GISSPA_CUDA(cudaGetLastError());       \
+  } while (0)
+
+// ---- complex arithmetic on float2 / double2
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+__host__ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__host__ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// multiply by +i (SIGN>0) or -i
+template <int SIGN>
+__host__ __device__ __forceinline__ float2 cmul_i(float2 a) {
+  return SIGN > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+// Order-preserving map of a float onto uint32 (larger float -> larger key).
+__device__ __forceinline__ uint32_t float_key(float f) {
+  uint32_t b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float key_float(uint32_t k) {
+  uint32_t b = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+  return __uint_as_float(b);
+}
+
+__device__ __forceinline__ unsigned brev8(unsigned v) { return __brev(v) >> 24; }
+
+// Exact shell index floor(hypot(a, b) + 0.5) - 1 evaluated in integers:
+// the k with k^2 - k < n <= k^2 + k, n = a^2 + b^2.
+__host__ __device__ __forceinline__ int shell_index(int a, int b) {
+  long long n = (long long)a * a + (long long)b * b;
+#ifdef __CUDA_ARCH__
+  long long k = (long long)floor(sqrt((double)n) + 0.5);
+#else
+  long long k = (long long)std::floor(std::sqrt((double)n) + 0.5);
+#endif
+  if (k > 0 && k * k - k >= n) --k;
+  if (k * k + k < n) ++k;
+  return (int)k - 1;
+}
+__host__ __device__ __forceinline__ int shell_xy(int x, int y, int nx, int ny) {
+  int a = y < ny - y ? y : ny - y;
+  int b = x < nx - x ? x : nx - x;
+  return shell_index(a, b);
+}
+
+// Storage types for the template-spectrum stream.
+struct SpecFp32 {
+  using T = float2;
+  __device__ __forceinline__ static float2 load(const T* p) { return *p; }
+  __device__ __forceinline__ static T pack(float2 v) { return v; }
+};
+struct SpecFp16 {
+  using T = __half2;
+  __device__ __forceinline__ static float2 load(const T* p) { return __half22float2(*p); }
+  __device__ __forceinline__ static T pack(float2 v) { return __float22half2_rn(v); }
+};
+struct SpecBf16 {
+  using T = __nv_bfloat162;
+  __device__ __forceinline__ static float2 load(const T* p) { return __bfloat1622float2(*p); }
+  __device__ __forceinline__ static T pack(float2 v) { return __float22bfloat162_rn(v); }
+};
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace gisspa

@@ -1,0 +1,394 @@
+// correlate.cu — pass A (multiply + column IFFT) and pass B (row C2R + epilogue).
+#include "../../include/gisspa.h"
+#include "correlate.cuh"
+#include "fft.cuh"
+
+namespace gisspa {
+namespace {
+
+struct BlockSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct WarpSync {
+  __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+
+template <int L>
+struct PassA;
+template <> struct PassA<256> { static constexpr int TT = 32, NC = 16; };
+template <> struct PassA<512> { static constexpr int TT = 64, NC = 8; };
+template <> struct PassA<1024> { static constexpr int TT = 64, NC = 4; };
+
+// Pass A: one team of TT threads per column slot, NC slots per CTA, one pair per blockIdx.y.
+template <int L, typename SPEC>
+__global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
+    pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
+                  int b0, int n0, int D, const float2* __restrict__ twL) {
+  constexpr int TT = PassA<L>::TT, NC = PassA<L>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
+  constexpr int PS = fft_padded_size(L);
+  __shared__ float2 smem[NC * PS];
+  const int team = threadIdx.x / TT, tid = threadIdx.x - team * TT;
+  const int c = blockIdx.x * NC + team;
+  const int p = blockIdx.y;
+  const int e = p / D, d = p - e * D;
+  const float2* Ib = I + (size_t)(b0 + e) * HS * L;
+  const typename SPEC::T* Tn = T + (size_t)(n0 + d) * HS * L;
+  float2 v[E];
+  if (c == 0) {
+    // columns kx = 0 and kx = L/2 have real inverse transforms: pack them as a + i b
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int ky = fft3_in_index<L, TT>(tid, i);
+      float2 a = cmulc(Ib[ky], SPEC::load(Tn + ky));
+      float2 b = cmulc(Ib[(size_t)NZ * L + ky], SPEC::load(Tn + (size_t)NZ * L + ky));
+      v[i] = make_float2(a.x - b.y, a.y + b.x);
+    }
+  } else {
+    const float2* Ic = Ib + (size_t)c * L;
+    const typename SPEC::T* Tc = Tn + (size_t)c * L;
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int ky = fft3_in_index<L, TT>(tid, i);
+      v[i] = cmulc(__ldg(Ic + ky), SPEC::load(Tc + ky));
+    }
+  }
+  fft3<L, TT, +1>(v, smem + team * PS, twL, tid, BlockSync{});
+  float2* Qp = Q + ((size_t)p * NZ + c) * L;
+#pragma unroll
+  for (int i = 0; i < E; ++i) Qp[fft3_out_index<L, TT>(tid, i)] = v[i];
+}
+
+template <int TEAM>
+__device__ __forceinline__ unsigned long long team_max_u64(unsigned long long k) {
+#pragma unroll
+  for (int off = TEAM / 2; off > 0; off >>= 1) {
+    unsigned long long o = __shfl_xor_sync(0xffffffffu, k, off, TEAM);
+    k = o > k ? o : k;
+  }
+  return k;
+}
+template <int TEAM>
+__device__ __forceinline__ double team_sum_f64(double x) {
+#pragma unroll
+  for (int off = TEAM / 2; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off, TEAM);
+  return x;
+}
+template <int TEAM>
+__device__ __forceinline__ bool team_any(bool pred) {
+  unsigned b = __ballot_sync(0xffffffffu, pred);
+  if constexpr (TEAM == 32) {
+    return b != 0;
+  } else {
+    const int sh = (threadIdx.x & 31) & ~(TEAM - 1);
+    return ((b >> sh) & ((1u << TEAM) - 1u)) != 0;
+  }
+}
+
+// Pass B: a team (TEAM lanes) per output row; RB rows per CTA, one window per blockIdx.y,
+// looping over the launch's D templates.
+template <int L, int TEAM, int RB, int NW, int EPI>
+__global__ void __launch_bounds__(NW * 32)
+    pass_b_kernel(CorrArgs a, const float2* __restrict__ twL, const float2* __restrict__ twNZ) {
+  constexpr int NZ = L / 2, E = NZ / TEAM, TPW = 32 / TEAM, NTEAM = NW * TPW, RPT = RB / NTEAM;
+  constexpr int RS = fft_padded_size(NZ);
+  static_assert(RB % NTEAM == 0, "rows must split evenly over teams");
+  static_assert(RB % 2 == 0, "float4 staging");
+  __shared__ float2 stage[RB * RS];
+  const int team = threadIdx.x / TEAM, lt = threadIdx.x - team * TEAM;
+  const int e = blockIdx.y, y0 = blockIdx.x * RB, win = a.b0 + e;
+  const float inv = 1.0f / (float)(L * L);
+  const size_t wbase = (size_t)win * L * L;
+
+  // per-lane pixel coordinates: element i, half h -> (out_y of row s, out_x)
+  int ox[E];
+#pragma unroll
+  for (int i = 0; i < E; ++i) ox[i] = (2 * fft3_out_index<NZ, TEAM>(lt, i) + L / 2) & (L - 1);
+
+  float acc1[RPT][E][2], acc2[RPT][E][2];
+  float best[(EPI == EPI_TOPK) ? RPT : 1][E][2];
+  int barg[(EPI == EPI_TOPK) ? RPT : 1][E][2];
+  float2 ms[(EPI == EPI_CHUNK) ? RPT : 1][E][2];
+  if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+#pragma unroll
+    for (int s = 0; s < RPT; ++s)
+#pragma unroll
+      for (int i = 0; i < E; ++i)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          acc1[s][i][h] = 0.f;
+          acc2[s][i][h] = 0.f;
+          if constexpr (EPI == EPI_TOPK) {
+            best[s][i][h] = -INFINITY;
+            barg[s][i][h] = -1;
+          }
+        }
+  }
+  if constexpr (EPI == EPI_CHUNK) {
+#pragma unroll
+    for (int s = 0; s < RPT; ++s) {
+      const int oy = (y0 + team + NTEAM * s + L / 2) & (L - 1);
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const float4 m = *reinterpret_cast<const float4*>(a.musig + wbase + (size_t)oy * L + ox[i]);
+        ms[s][i][0] = make_float2(m.x, m.y);
+        ms[s][i][1] = make_float2(m.z, m.w);
+      }
+    }
+  }
+
+  for (int d = 0; d < a.D; ++d) {
+    const int p = e * a.D + d;
+    const float2* Qp = a.Q + (size_t)p * NZ * L;
+    __syncthreads();
+    constexpr int UPC = RB / 2;
+    for (int u = threadIdx.x; u < NZ * UPC; u += NW * 32) {
+      const int c = u / UPC, yy = (u - c * UPC) * 2;
+      const float4 q = __ldg(reinterpret_cast<const float4*>(Qp + (size_t)c * L + y0 + yy));
+      stage[yy * RS + c] = make_float2(q.x, q.y);
+      stage[(yy + 1) * RS + c] = make_float2(q.z, q.w);
+    }
+    __syncthreads();
+    double nn_s1 = 0.0, nn_s2 = 0.0;
+#pragma unroll
+    for (int s = 0; s < RPT; ++s) {
+      const int r = team + NTEAM * s;
+      const int oy = (y0 + r + L / 2) & (L - 1);
+      float2* row = stage + r * RS;
+      float2 v[E];
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const int k = fft3_in_index<NZ, TEAM>(lt, i);
+        float2 xk, xm;
+        if (k == 0) {
+          const float2 q = row[0];
+          xk = make_float2(q.x, 0.f);
+          xm = make_float2(q.y, 0.f);
+        } else {
+          xk = row[k];
+          xm = row[NZ - k];
+        }
+        const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
+        const float2 od = make_float2(xk.x - xm.x, xk.y + xm.y);
+        float2 w = __ldg(twL + k);
+        w.y = -w.y;
+        const float2 o = cmul(w, od);
+        v[i] = make_float2(ev.x - o.y, ev.y + o.x);
+      }
+      __syncwarp();
+      fft3<NZ, TEAM, +1>(v, row, twNZ, lt, WarpSync{});
+
+      if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+#pragma unroll
+        for (int i = 0; i < E; ++i)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const float c = (h ? v[i].y : v[i].x) * inv;
+            acc1[s][i][h] += c;
+            acc2[s][i][h] = fmaf(c, c, acc2[s][i][h]);
+            if constexpr (EPI == EPI_TOPK) {
+              if (c > best[s][i][h]) {
+                best[s][i][h] = c;
+                barg[s][i][h] = a.angle * a.nt_total + a.n0 + d;
+              }
+            }
+          }
+      } else if constexpr (EPI == EPI_CHUNK) {
+        float z[E][2];
+        float zmax = -INFINITY;
+#pragma unroll
+        for (int i = 0; i < E; ++i)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const float c = (h ? v[i].y : v[i].x) * inv;
+            z[i][h] = (c - ms[s][i][h].x) * ms[s][i][h].y;
+            zmax = fmaxf(zmax, z[i][h]);
+          }
+        if (team_any<TEAM>(zmax >= a.thresh)) {
+          constexpr int CPR = L >= 256 ? L / 256 : 1;  // chunks per row
+#pragma unroll
+          for (int ch = 0; ch < CPR; ++ch) {
+            unsigned long long key = 0;
+#pragma unroll
+            for (int i = 0; i < E; ++i)
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                const int x = ox[i] + h;
+                if ((x >> 8) != ch) continue;
+                const int t = (oy * L + x) & 255;
+                const unsigned long long k2 =
+                    ((unsigned long long)float_key(z[i][h]) << 32) | (unsigned)(255 - brev8(t));
+                key = k2 > key ? k2 : key;
+              }
+            key = team_max_u64<TEAM>(key);
+            if (lt == 0) {
+              const float zb = key_float((uint32_t)(key >> 32));
+              if (zb >= a.thresh) {
+                const int t = brev8(255 - (unsigned)(key & 0xffu));
+                const int id = ((oy * L + ch * 256) & ~255) + t;
+                const int px = id % L, py = id / L;
+                const int cx = a.offx[win % a.bx] + px, cy = a.offy[win / a.bx] + py;
+                if (cx >= a.dmin && cx < a.nx - a.dmin && cy >= a.dmin && cy < a.ny - a.dmin) {
+                  const unsigned slot = atomicAdd(a.cand_count, 1u);
+                  if (slot < a.cand_cap) {
+                    Cand cd;
+                    cd.score = zb;
+                    cd.x = px;
+                    cd.y = py;
+                    cd.window = win;
+                    cd.templ = a.n0 + d;
+                    cd.angle = a.angle;
+                    cd.chunk = id >> 8;
+                    cd.pad = 0;
+                    a.cand[slot] = cd;
+                  }
+                }
+              }
+            }
+          }
+        }
+      } else if constexpr (EPI == EPI_NONORM) {
+        constexpr int CPR = L >= 256 ? L / 256 : 1;
+        // get_peak_and_SUM (kernels.cu:725-763): sums over every pixel, max with the
+        // border (closer than diameter/4 to the window edge) forced to 0
+#pragma unroll
+        for (int i = 0; i < E; ++i) {
+          nn_s1 += (double)v[i].x + (double)v[i].y;
+          nn_s2 += (double)v[i].x * v[i].x + (double)v[i].y * v[i].y;
+        }
+#pragma unroll
+        for (int ch = 0; ch < CPR; ++ch) {
+          unsigned long long key = 0;
+#pragma unroll
+          for (int i = 0; i < E; ++i)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int x = ox[i] + h;
+              if ((x >> 8) != ch) continue;
+              float val = h ? v[i].y : v[i].x;
+              if (x < a.border || x > L - a.border || oy < a.border || oy > L - a.border) val = 0.f;
+              const int t = (oy * L + x) & 255;
+              const unsigned long long k2 =
+                  ((unsigned long long)float_key(val) << 32) | (unsigned)(255 - brev8(t));
+              key = k2 > key ? k2 : key;
+            }
+          key = team_max_u64<TEAM>(key);
+          if (lt == 0) {
+            const float vb = key_float((uint32_t)(key >> 32));
+            if (vb > 0.f) {
+              const int t = brev8(255 - (unsigned)(key & 0xffu));
+              const int chunk = ((oy * L + ch * 256) >> 8);
+              const unsigned long long g =
+                  ((unsigned long long)float_key(vb) << 32) | ((unsigned long long)(0xFFFFFu - chunk) << 8) | t;
+              atomicMax(a.nn_key + (size_t)win * a.nt_total + a.n0 + d, g);
+            }
+          }
+        }
+      } else if constexpr (EPI == EPI_MAP) {
+        float* out = a.map_out + (size_t)p * L * L + (size_t)oy * L;
+#pragma unroll
+        for (int i = 0; i < E; ++i)
+          *reinterpret_cast<float2*>(out + ox[i]) = make_float2(v[i].x * inv, v[i].y * inv);
+      }
+    }
+    if constexpr (EPI == EPI_NONORM) {
+      nn_s1 = team_sum_f64<TEAM>(nn_s1);
+      nn_s2 = team_sum_f64<TEAM>(nn_s2);
+      if (lt == 0) {
+        const size_t q = (size_t)win * a.nt_total + a.n0 + d;
+        atomicAdd(a.nn_sum + 2 * q, nn_s1);
+        atomicAdd(a.nn_sum + 2 * q + 1, nn_s2);
+      }
+    }
+  }
+
+  if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+#pragma unroll
+    for (int s = 0; s < RPT; ++s) {
+      const int oy = (y0 + team + NTEAM * s + L / 2) & (L - 1);
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const size_t pix = wbase + (size_t)oy * L + ox[i];
+        double2* p1 = reinterpret_cast<double2*>(a.S1 + pix);
+        double2* p2 = reinterpret_cast<double2*>(a.S2 + pix);
+        double2 s1 = *p1, s2 = *p2;
+        s1.x += acc1[s][i][0];
+        s1.y += acc1[s][i][1];
+        s2.x += acc2[s][i][0];
+        s2.y += acc2[s][i][1];
+        *p1 = s1;
+        *p2 = s2;
+        if constexpr (EPI == EPI_TOPK) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+            if (barg[s][i][h] >= 0 && best[s][i][h] > a.cmax[pix + h]) {
+              a.cmax[pix + h] = best[s][i][h];
+              a.carg[pix + h] = barg[s][i][h];
+            }
+        }
+      }
+    }
+  }
+}
+
+template <int L, typename SPEC>
+void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
+              const float2* twL, cudaStream_t s) {
+  constexpr int NZ = L / 2;
+  dim3 grid(NZ / PassA<L>::NC, cl.E * cl.D);
+  pass_a_kernel<L, SPEC><<<grid, PassA<L>::TT * PassA<L>::NC, 0, s>>>(
+      I, static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL);
+  GISSPA_LAUNCH_CHECK();
+}
+
+template <int L, int TEAM, int RB, int NW, int EPI>
+void launch_b_cfg(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ,
+                  cudaStream_t s) {
+  dim3 grid(L / RB, cl.E);
+  pass_b_kernel<L, TEAM, RB, NW, EPI><<<grid, NW * 32, 0, s>>>(args, twL, twNZ);
+  GISSPA_LAUNCH_CHECK();
+}
+
+template <int L, int TEAM, int NW>
+void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ, cudaStream_t s) {
+  constexpr int NT = NW * (32 / TEAM);
+  switch (cl.epi) {
+    case EPI_SUM: launch_b_cfg<L, TEAM, (L == 512 ? 2 * NT : NT), NW, EPI_SUM>(cl, args, twL, twNZ, s); break;
+    case EPI_CHUNK: launch_b_cfg<L, TEAM, NT, NW, EPI_CHUNK>(cl, args, twL, twNZ, s); break;
+    case EPI_TOPK: launch_b_cfg<L, TEAM, NT, NW, EPI_TOPK>(cl, args, twL, twNZ, s); break;
+    case EPI_NONORM: launch_b_cfg<L, TEAM, NT, NW, EPI_NONORM>(cl, args, twL, twNZ, s); break;
+    case EPI_MAP: launch_b_cfg<L, TEAM, NT, NW, EPI_MAP>(cl, args, twL, twNZ, s); break;
+    default: throw CudaError{cudaErrorInvalidValue, "unknown epilogue"};
+  }
+}
+
+template <int L, int TEAM, int NW>
+int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
+                const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {
+  if (ev) GISSPA_CUDA(cudaEventRecord(ev[0], s));
+  switch (cl.spec) {
+    case GISSPA_SPEC_FP32: launch_a<L, SpecFp32>(cl, I, T, Q, args, twL, s); break;
+    case GISSPA_SPEC_FP16: launch_a<L, SpecFp16>(cl, I, T, Q, args, twL, s); break;
+    case GISSPA_SPEC_BF16: launch_a<L, SpecBf16>(cl, I, T, Q, args, twL, s); break;
+    default: throw CudaError{cudaErrorInvalidValue, "unknown spectrum precision"};
+  }
+  if (ev) GISSPA_CUDA(cudaEventRecord(ev[1], s));
+  launch_b<L, TEAM, NW>(cl, args, twL, twNZ, s);
+  if (ev) GISSPA_CUDA(cudaEventRecord(ev[2], s));
+  return 2;
+}
+
+}  // namespace
+
+bool correlate_supported(int L) { return L == 256 || L == 512 || L == 1024; }
+
+int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
+                     const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {
+  switch (cl.L) {
+    case 256: return launch_pair<256, 16, 8>(cl, I, T, Q, args, twL, twNZ, s, ev);
+    case 512: return launch_pair<512, 32, 8>(cl, I, T, Q, args, twL, twNZ, s, ev);
+    case 1024: return launch_pair<1024, 32, 8>(cl, I, T, Q, args, twL, twNZ, s, ev);
+    default: throw CudaError{cudaErrorInvalidValue, "window size without correlation kernels"};
+  }
+}
+
+}  // namespace gisspa

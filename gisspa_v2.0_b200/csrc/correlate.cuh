@@ -1,0 +1,85 @@
+// correlate.cuh — the hot loop: fused conjugate multiply + 2D C2R inverse FFT +
+// per-pixel epilogue for a batch of (window, template) pairs at one angle.
+//
+// Spectra are stored as half spectra in column-major order, S[kx][ky] with
+// kx in [0, L/2] and ky in [0, L) ("kx-major"), the layout the column pass reads.
+//   pass A: for every pair and column kx: Z[ky] = I[kx][ky] conj(T[kx][ky]);
+//           columns 0 and L/2 (whose inverse transforms are real) are packed into
+//           one complex column; inverse FFT of length L along ky -> Q[pair][kx][y].
+//   pass B: per output row y, a length-L/2 complex inverse FFT turns the L/2+1
+//           Hermitian-half values into L real samples (even/odd interleave);
+//           the zero lag is moved to (L/2, L/2) (the reference's (-1)^(kx+ky)
+//           factor, kernels.cu:668-677) and the epilogue consumes the row.
+// The result equals Re(IFFT2(I conj(T) (-1)^(kx+ky))) of the reference
+// (compute_corner_CCG kernels.cu:645-678 + cufftExecC2C norm.cu:536/568).
+#pragma once
+
+#include "common.cuh"
+
+namespace gisspa {
+
+enum Epilogue : int {
+  EPI_SUM = 0,     // sweep 1: S1 += c, S2 += c^2 (c = CC / L^2), FP64 state
+  EPI_CHUNK = 1,   // sweep 2: z = (c - mu) / sigma, 256-pixel chunk max, threshold -> candidates
+  EPI_TOPK = 2,    // one sweep: S1, S2 and per-pixel max c with its (angle, template)
+  EPI_NONORM = 3,  // norm_type=0: per pair peak (border zeroed), sum, sum of squares of CC
+  EPI_MAP = 4      // write c maps (tests and the no-scratch entry point)
+};
+
+// A picked chunk (or, for EPI_NONORM, nothing: per-pair reductions go to nn_*).
+struct Cand {
+  float score;
+  int x, y;          // window-local pixel (zero lag at L/2)
+  int window, templ, angle, chunk;
+  int pad;
+};
+
+struct CorrArgs {
+  const float2* Q;          // pass A output, [pairs][L/2][L]
+  int D;                    // templates per window in this launch
+  int b0, n0;               // first window / template of the launch
+  int angle;                // index of the angle in the angle sequence
+  int nt_real;              // templates >= nt_real never produce picks
+  int nt_total;             // N_T used in the (angle, template) combination index
+  // EPI_SUM / EPI_TOPK state, [W][L][L]
+  double* S1;
+  double* S2;
+  float* cmax;
+  int* carg;
+  // EPI_CHUNK
+  const float2* musig;      // [W][L][L] (mu, 1/sigma or 0)
+  float thresh;
+  const int* offx;          // window offsets (x of window b % bx), (y of window b / bx)
+  const int* offy;
+  int bx, nx, ny;
+  float dmin;               // centre must lie in [dmin, n - dmin)
+  Cand* cand;
+  unsigned* cand_count;
+  unsigned cand_cap;
+  // EPI_NONORM, indexed [window][template] with nt_total templates per window
+  unsigned long long* nn_key;
+  double* nn_sum;           // [W][nt_total][2]
+  float border;             // diameter / 4
+  // EPI_MAP, [pairs][L][L]
+  float* map_out;
+};
+
+struct CorrLaunch {
+  int L;
+  int E;              // windows in this launch
+  int D;              // templates per window in this launch
+  int spec;           // GISSPA_SPEC_*
+  int epi;            // Epilogue
+};
+
+// Launch pass A then pass B on stream s.  I: window spectra [W][L/2+1][L];
+// T: template spectra [N][L/2+1][L] in the storage type of `spec`; Q: scratch.
+// Returns the number of kernel launches issued.
+// ev (optional): three events recorded before pass A, between the passes and after pass B.
+int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
+                     const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev = nullptr);
+
+// Whether a window size has compiled correlation kernels.
+bool correlate_supported(int L);
+
+}  // namespace gisspa

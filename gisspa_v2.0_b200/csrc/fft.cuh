@@ -1,0 +1,174 @@
+// fft.cuh — register/shared-memory Stockham FFT building blocks (sm_100a).
+//
+// A transform of length N is spread over a team of T threads, each holding
+// E = N/T complex points in registers.  Every stage of radix R runs E/R
+// butterflies per thread; stage boundaries exchange data through a padded
+// shared-memory buffer (pad(i) = i + i/16 keeps the strided Stockham stores
+// free of bank conflicts for the radices used here).  Stockham ordering needs no
+// bit reversal: stage inputs are x[j + m N/R], outputs go to
+// y[(j/Ns) Ns R + (j mod Ns) + r Ns], j = tid + T q.
+//
+// SIGN = -1 is the forward transform, +1 the inverse (unnormalised), matching the
+// cuFFT convention the reference relies on.
+#pragma once
+
+#include "common.cuh"
+
+namespace gisspa {
+
+__host__ __device__ constexpr int fft_pad(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int fft_padded_size(int n) { return n + (n >> 4) + 1; }
+
+// Multiply v by W_R^K = exp(SIGN * 2 pi i K / R) with exact special cases.
+template <int R, int K, int SIGN>
+__device__ __forceinline__ float2 mul_wr(float2 v) {
+  constexpr int KK = K % R;
+  if constexpr (KK == 0) {
+    return v;
+  } else if constexpr (4 * KK == R) {
+    return cmul_i<SIGN>(v);
+  } else if constexpr (2 * KK == R) {
+    return make_float2(-v.x, -v.y);
+  } else if constexpr (4 * KK == 3 * R) {
+    return cmul_i<-SIGN>(v);
+  } else if constexpr (8 * KK == R) {
+    constexpr float h = 0.70710678118654752440f;
+    return make_float2(h * (v.x - SIGN * v.y), h * (v.y + SIGN * v.x));
+  } else if constexpr (8 * KK == 3 * R) {
+    constexpr float h = 0.70710678118654752440f;
+    return make_float2(h * (-v.x - SIGN * v.y), h * (-v.y + SIGN * v.x));
+  } else {
+    // R == 16, odd K: angles k * pi / 8
+    constexpr double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;
+    constexpr int k8 = (16 / R) * KK;  // in units of 2 pi / 16
+    constexpr double cc = (k8 == 1) ? c1 : (k8 == 3) ? s1 : (k8 == 5) ? -s1 : -c1;
+    constexpr double ss = (k8 == 1) ? s1 : (k8 == 3) ? c1 : (k8 == 5) ? c1 : s1;
+    constexpr float c = (float)cc, s = (float)(SIGN * ss);
+    return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
+  }
+}
+
+// In-register DFT of length R (R in {1, 2, 4, 8, 16}), natural order in and out.
+template <int R, int SIGN>
+struct Dft {
+  template <int K = 0>
+  __device__ __forceinline__ static void combine(float2* a, const float2* e, const float2* o) {
+    if constexpr (K < R / 2) {
+      float2 t = mul_wr<R, K, SIGN>(o[K]);
+      a[K] = cadd(e[K], t);
+      a[K + R / 2] = csub(e[K], t);
+      combine<K + 1>(a, e, o);
+    }
+  }
+  __device__ __forceinline__ static void run(float2* a) {
+    if constexpr (R == 1) {
+      return;
+    } else if constexpr (R == 2) {
+      float2 t = a[1];
+      a[1] = csub(a[0], t);
+      a[0] = cadd(a[0], t);
+    } else {
+      float2 e[R / 2], o[R / 2];
+#pragma unroll
+      for (int m = 0; m < R / 2; ++m) {
+        e[m] = a[2 * m];
+        o[m] = a[2 * m + 1];
+      }
+      Dft<R / 2, SIGN>::run(e);
+      Dft<R / 2, SIGN>::run(o);
+      combine<0>(a, e, o);
+    }
+  }
+};
+
+// Twiddle W_N^p for the stage, from a table of exp(-2 pi i p / N), p < N.
+template <int SIGN>
+__device__ __forceinline__ float2 table_tw(const float2* __restrict__ tw, int p) {
+  float2 w = __ldg(tw + p);
+  return SIGN > 0 ? make_float2(w.x, -w.y) : w;
+}
+
+// One Stockham stage: v holds this thread's inputs as v[q*R + m] = x[j_q + m N/R].
+// Twiddles, butterflies, and (unless LAST) stores to shared memory.
+template <int N, int T, int R, int NS, int SIGN, bool LAST>
+__device__ __forceinline__ void stockham_stage(float2* v, float2* sm, const float2* __restrict__ tw, int tid) {
+  constexpr int E = N / T, B = E / R;
+  static_assert(E % R == 0, "radix must divide the points per thread");
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    const int j = tid + T * q;
+    const int k = j & (NS - 1);
+    float2* a = v + q * R;
+    if constexpr (NS > 1) {
+      constexpr int step = N / (NS * R);
+#pragma unroll
+      for (int m = 1; m < R; ++m) a[m] = cmul(a[m], table_tw<SIGN>(tw, k * m * step));
+    }
+    Dft<R, SIGN>::run(a);
+    if constexpr (!LAST) {
+      const int base = (j / NS) * NS * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) sm[fft_pad(base + r * NS)] = a[r];
+    }
+  }
+}
+
+// Load the inputs of the next stage (radix R) from shared memory.
+template <int N, int T, int R>
+__device__ __forceinline__ void stockham_load(float2* v, const float2* sm, int tid) {
+  constexpr int E = N / T, B = E / R;
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    const int j = tid + T * q;
+#pragma unroll
+    for (int m = 0; m < R; ++m) v[q * R + m] = sm[fft_pad(j + m * (N / R))];
+  }
+}
+
+// Radix plans: three stages for every length used by the correlation kernels.
+//   first stage inputs of thread tid:  x[tid + T q + m N/R1]
+//   last stage outputs of thread tid:  y[j + r N/R3], j = tid + T q
+template <int N, int T>
+struct Plan;
+template <> struct Plan<256, 32> { static constexpr int R1 = 8, R2 = 8, R3 = 4; };
+template <> struct Plan<512, 64> { static constexpr int R1 = 8, R2 = 8, R3 = 8; };
+template <> struct Plan<512, 32> { static constexpr int R1 = 16, R2 = 8, R3 = 4; };
+template <> struct Plan<1024, 64> { static constexpr int R1 = 16, R2 = 16, R3 = 4; };
+template <> struct Plan<128, 32> { static constexpr int R1 = 4, R2 = 8, R3 = 4; };
+template <> struct Plan<128, 16> { static constexpr int R1 = 8, R2 = 4, R3 = 4; };
+
+// Full three-stage transform.  v: E inputs in first-stage order; on return v holds
+// the outputs in last-stage order.  sm: this team's padded buffer; SYNC() must be a
+// barrier covering the team (warp or block).  The buffer is free again on return.
+template <int N, int T, int SIGN, typename Sync>
+__device__ __forceinline__ void fft3(float2* v, float2* sm, const float2* __restrict__ tw, int tid, Sync sync) {
+  using P = Plan<N, T>;
+  constexpr int R1 = P::R1, R2 = P::R2, R3 = P::R3;
+  static_assert(R1 * R2 * R3 == N, "plan must factor N");
+  stockham_stage<N, T, R1, 1, SIGN, false>(v, sm, tw, tid);
+  sync();
+  stockham_load<N, T, R2>(v, sm, tid);
+  sync();
+  stockham_stage<N, T, R2, R1, SIGN, false>(v, sm, tw, tid);
+  sync();
+  stockham_load<N, T, R3>(v, sm, tid);
+  sync();
+  stockham_stage<N, T, R3, R1 * R2, SIGN, true>(v, sm, tw, tid);
+}
+
+// Index of output element e (0 <= e < E) held by thread tid after fft3.
+template <int N, int T>
+__device__ __forceinline__ int fft3_out_index(int tid, int e) {
+  constexpr int R3 = Plan<N, T>::R3;
+  const int q = e / R3, r = e % R3;
+  return tid + T * q + r * (N / R3);
+}
+// Index of input element e held by thread tid before fft3.
+template <int N, int T>
+__device__ __forceinline__ int fft3_in_index(int tid, int e) {
+  constexpr int R1 = Plan<N, T>::R1;
+  const int q = e / R1, m = e % R1;
+  return tid + T * q + m * (N / R1);
+}
+
+}  // namespace gisspa

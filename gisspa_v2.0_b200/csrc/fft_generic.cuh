@@ -1,0 +1,72 @@
+// fft_generic.cuh — batched 1D/2D complex FFTs for every size outside the hot loop
+// (template and image preparation, window spectra, per-angle template spectra).
+//
+// Power-of-two lengths up to 16384 run one shared-memory transform per row; other
+// lengths use Bluestein's chirp-z algorithm on top of it.  2D transforms are
+// rows -> transpose -> rows (-> transpose).  All transforms are unnormalised.
+#pragma once
+
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+namespace gisspa {
+
+// Grow-only device buffer.
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+  ~DevBuf() { release(); }
+  void* ensure(size_t bytes) {
+    if (bytes > n_) {
+      release();
+      GISSPA_CUDA(cudaMalloc(&p_, bytes));
+      n_ = bytes;
+    }
+    return p_;
+  }
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  template <typename T>
+  T* as() const { return static_cast<T*>(p_); }
+  size_t size() const { return n_; }
+
+ private:
+  void* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+class FftEngine {
+ public:
+  // Table of exp(-2 pi i p / n), p < n, n a power of two (device pointer, cached).
+  const float2* twiddles(int n);
+  // In-place transform of `rows` contiguous rows of length n (any n >= 1).
+  void rows(float2* data, long long rows, int n, int sign, float scale, cudaStream_t s);
+  // out[b][c][r] = in[b][r][c] for rows x cols matrices; optional row subset
+  // [0, out_rows) of the transposed result (i.e. input columns [0, out_rows)).
+  void transpose(const float2* in, float2* out, int batch, int rows, int cols, cudaStream_t s, int out_rows = -1);
+  // In-place 2D transform of batch x ny x nx, using tmp (same size) as scratch.
+  void fft2(float2* data, float2* tmp, int batch, int ny, int nx, int sign, float scale, cudaStream_t s);
+
+ private:
+  struct Blue {
+    int n = 0, m = 0;
+    DevBuf chirp, bfwd, binv;
+  };
+  Blue& bluestein(int n);
+  std::map<int, DevBuf> tw_;
+  std::map<int, std::unique_ptr<Blue>> blue_;
+  DevBuf scratch_;
+};
+
+bool is_pow2(long long n);
+
+}  // namespace gisspa

@@ -1,0 +1,806 @@
+// search.cu — per-micrograph orchestration of the search (SearchNorm::work,
+// norm.cu:620-660; SearchNoNorm::work, nonorm.cu:559-589) on one stream.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "correlate.cuh"
+#include "prep.cuh"
+#include "search.cuh"
+
+namespace gisspa {
+
+std::vector<int> window_offsets(int len, int l, int ov) {
+  std::vector<int> off{0};
+  int o = 0;
+  while (o + l < len) {
+    o += l - ov;
+    if (o + l >= len) o = len - l;
+    off.push_back(o);
+  }
+  return off;
+}
+
+int window_count_nonorm(int len, int l, int ov) {
+  int o = 0, n = 1;
+  while (o + l < len) {
+    o += l - ov;
+    if (o + l >= len) o = len - l;
+    ++n;
+  }
+  return n;
+}
+
+std::vector<float> angle_list(float step) {
+  std::vector<float> a;
+  for (float e = 0.0f; e < 360.0f; e += step) a.push_back(e);
+  return a;
+}
+
+int validate_config(const gisspa_config& c, std::string& err) {
+  const int l = c.window_size;
+  if (l <= 0 || l % 16) {
+    err = "window_size " + std::to_string(l) + " must be a positive multiple of 16";
+    return GISSPA_ERR_SHAPE;
+  }
+  if (!correlate_supported(l)) {
+    err = "window_size " + std::to_string(l) + " is not built (supported: 256, 512, 1024)";
+    return GISSPA_ERR_UNSUPPORTED;
+  }
+  if (c.overlap < 0 || c.overlap >= l) {
+    err = "overlap must lie in [0, window_size)";
+    return GISSPA_ERR_SHAPE;
+  }
+  if (!(c.phistep > 0) || c.phistep > 360) {
+    err = "phistep must lie in (0, 360]";
+    return GISSPA_ERR_ARG;
+  }
+  if (!(c.angpix > 0) || !(c.energy > 0) || !(c.highres > 0) || c.kk < 0 || c.diameter < 0) {
+    err = "angpix, energy, Highres must be positive and kk, diameter non-negative";
+    return GISSPA_ERR_ARG;
+  }
+  if (c.spectrum_precision < 0 || c.spectrum_precision > 2) {
+    err = "unknown spectrum_precision";
+    return GISSPA_ERR_ARG;
+  }
+  if (c.pick_mode != GISSPA_PICK_CHUNK && c.pick_mode != GISSPA_PICK_TOPK) {
+    err = "unknown pick_mode";
+    return GISSPA_ERR_ARG;
+  }
+  if (c.pick_mode == GISSPA_PICK_TOPK && (c.topk <= 0 || c.exclusion_radius < 0)) {
+    err = "topk must be positive and exclusion_radius non-negative";
+    return GISSPA_ERR_ARG;
+  }
+  if (c.norm_type == 0 && c.pick_mode == GISSPA_PICK_TOPK) {
+    err = "top-K picking is defined for norm_type=1 only";
+    return GISSPA_ERR_UNSUPPORTED;
+  }
+  if (c.norm_type == 0 && c.tile_size <= 0) {
+    err = "tile_size must be positive";
+    return GISSPA_ERR_ARG;
+  }
+  if (c.template_batch < 0 || c.window_batch < 0) {
+    err = "template_batch and window_batch must be >= 0";
+    return GISSPA_ERR_ARG;
+  }
+  return GISSPA_OK;
+}
+
+int validate_image(const gisspa_config& c, int nx, int ny, std::string& err) {
+  if (nx <= 0 || ny <= 0 || nx > 65536 || ny > 65536) {
+    err = "image size " + std::to_string(nx) + "x" + std::to_string(ny) + " out of range";
+    return GISSPA_ERR_SHAPE;
+  }
+  if (c.norm_type == 0 && (nx < c.tile_size || ny < c.tile_size)) {
+    // TileImages copies tile_size rows of tile_size floats (tileimages.cpp:61-65)
+    err = "norm_type=0 needs an image of at least tile_size x tile_size";
+    return GISSPA_ERR_SHAPE;
+  }
+  if (std::max(nx, ny) / 2 > (1 << 15)) {
+    err = "image too large for the radial shell tables";
+    return GISSPA_ERR_SHAPE;
+  }
+  return GISSPA_OK;
+}
+
+namespace {
+
+template <typename T>
+T* buf(DevBuf& b, size_t count) {
+  return static_cast<T*>(b.ensure(sizeof(T) * std::max<size_t>(count, 1)));
+}
+
+size_t spec_bytes(int spec) { return spec == GISSPA_SPEC_FP32 ? sizeof(float2) : sizeof(__half2); }
+
+__global__ void musig_kernel(const double* __restrict__ S1, const double* __restrict__ S2, long long n, double N,
+                             float2* __restrict__ ms) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  // set_CCG_mean (kernels.cu:697-706) in FP64; update_CCG uses z = 0 when sigma <= 0 (kernels.cu:720)
+  const double mu = S1[i] / N;
+  const double sd = sqrt(S2[i] / N - mu * mu);
+  ms[i] = make_float2((float)mu, sd > 0 ? (float)(1.0 / sd) : 0.f);
+}
+
+__global__ void fill_kernel(float* __restrict__ a, int* __restrict__ b, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a[i] = -INFINITY;
+  b[i] = -1;
+}
+
+// Top-K: image map of the max z over windows covering each pixel (ties: lowest window).
+__global__ void zmap_kernel(const float* __restrict__ cmax, const int* __restrict__ carg,
+                            const float2* __restrict__ ms, int l, const int* __restrict__ offx,
+                            const int* __restrict__ offy, int bx, int nx, int ny,
+                            unsigned long long* __restrict__ zkey) {
+  const int b = blockIdx.y;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= l * l) return;
+  const size_t i = (size_t)b * l * l + k;
+  if (carg[i] < 0) return;
+  const float2 m = ms[i];
+  const float z = (cmax[i] - m.x) * m.y;
+  const int cx = offx[b % bx] + k % l, cy = offy[b / bx] + k / l;
+  if (cx >= nx || cy >= ny) return;
+  const unsigned long long key = ((unsigned long long)float_key(z) << 32) | (unsigned)(0xFFFFFFFFu - (unsigned)b);
+  atomicMax(zkey + (size_t)cy * nx + cx, key);
+}
+
+struct ZCand {
+  float z;
+  int q, win, arg;
+};
+
+__global__ void zcompact_kernel(const unsigned long long* __restrict__ zkey, int nx, int ny, float thresh, float dmin,
+                                const int* __restrict__ carg, int l, const int* __restrict__ offx,
+                                const int* __restrict__ offy, int bx, ZCand* __restrict__ out,
+                                unsigned* __restrict__ count, unsigned cap) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)nx * ny) return;
+  const unsigned long long k = zkey[q];
+  if (!k) return;
+  const float z = key_float((uint32_t)(k >> 32));
+  const int x = (int)(q % nx), y = (int)(q / nx);
+  if (!(z >= thresh) || x < dmin || x >= nx - dmin || y < dmin || y >= ny - dmin) return;
+  const int b = (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFu));
+  const int px = x - offx[b % bx], py = y - offy[b / bx];
+  const unsigned s = atomicAdd(count, 1u);
+  if (s < cap) out[s] = ZCand{z, (int)q, b, carg[(size_t)b * l * l + (size_t)py * l + px]};
+}
+
+struct Ctx {
+  gisspa_handle* h;
+  cudaStream_t s;
+  int l;
+  long long L2;
+  DevParams p;
+};
+
+// ---- template preparation (PreprocessTemplate norm.cu:194-354 / nonorm.cu:178-344)
+void prepare_templates(Ctx& c) {
+  gisspa_handle* h = c.h;
+  const int l = c.l, nt = h->nt;
+  const bool nonorm = h->cfg.norm_type == 0;
+  float2* tb = buf<float2>(h->tb, (size_t)nt * c.L2);
+  float2* tmp = buf<float2>(h->tb_tmp, (size_t)nt * c.L2);
+  tmpl_pad(h->d_stack.as<float>(), nt, h->tw, h->th, l, tb, c.s);
+  tmpl_edge_normalise(tb, nt, l, nullptr, c.s);
+  h->fft.fft2(tb, tmp, nt, l, l, -1, 1.0f / (float)c.L2, c.s);
+  const int nb = l / 2;
+  double* ra = buf<double>(h->ra, (size_t)nt * nb);
+  unsigned* rb = buf<unsigned>(h->rb, nb);
+  radial_power(tb, nt, l, l, ra, rb, nb, c.s);
+  tmpl_whiten(tb, nt, l, ra, rb, nb, c.s);
+  if (nonorm) {  // nonorm.cu:291-299: IFFT, real-space mask, FFT / l^2
+    h->fft.fft2(tb, tmp, nt, l, l, +1, 1.f, c.s);
+    mask_real(tb, nt, l, h->cfg.diameter, h->cfg.edge_half_width, c.s);
+    h->fft.fft2(tb, tmp, nt, l, l, -1, 1.0f / (float)c.L2, c.s);
+  }
+  float* table = buf<float>(h->table, c.L2);
+  tmpl_weight_table(table, l, c.p, c.s);
+  apply_table(tb, nt, l, table, c.s);
+  rms_normalise(tb, nt, l, nullptr, c.s);
+  if (!nonorm) {
+    h->fft.fft2(tb, tmp, nt, l, l, +1, 1.f, c.s);  // norm.cu:350-351, unnormalised
+    real_part(tb, buf<float>(h->prep_real, (size_t)nt * c.L2), (long long)nt * c.L2, 1.f, c.s);
+  } else {
+    h->fft.transpose(tb, tmp, nt, l, l, c.s, l / 2 + 1);
+    void* ts = h->tspec.ensure(spec_bytes(h->cfg.spectrum_precision) * (size_t)nt * (l / 2 + 1) * l);
+    finalize_spectra(tmp, nt, l, nullptr, h->cfg.spectrum_precision, ts, 1.0, c.s);
+  }
+}
+
+// ---- micrograph preparation (LoadImage norm.cu:156-181 + PreprocessImage norm.cu:356-402)
+void preprocess_full(Ctx& c, float2* G, int nx, int ny, bool zero_dc) {
+  gisspa_handle* h = c.h;
+  const long long N = (long long)nx * ny;
+  float2* tmp = buf<float2>(h->img_tmp, N);
+  h->fft.fft2(G, tmp, 1, ny, nx, -1, (float)(1.0 / (double)N), c.s);
+  phase_flip(G, nx, ny, c.p, c.s);
+  const int nb = std::max(nx, ny) / 2;
+  double* ra = buf<double>(h->ra, std::max<size_t>((size_t)h->nt * (c.l / 2), nb));
+  unsigned* rb = buf<unsigned>(h->rb, std::max(nb, c.l / 2));
+  radial_power(G, 1, nx, ny, ra, rb, nb, c.s);
+  image_filter(G, nx, ny, c.p, ra, rb, nb, zero_dc, c.s);
+  h->fft.fft2(G, tmp, 1, ny, nx, +1, 1.f, c.s);
+}
+
+// SplitImage (norm.cu:404-477): windows -> FFT / l^2 -> radial RMS -> kx-major half spectra.
+void window_spectra(Ctx& c, const float* img, int nx, int ny, const std::vector<int>& ox, const std::vector<int>& oy) {
+  gisspa_handle* h = c.h;
+  const int l = c.l, bx = (int)ox.size(), W = bx * (int)oy.size();
+  int* dox = buf<int>(h->offx, ox.size());
+  int* doy = buf<int>(h->offy, oy.size());
+  GISSPA_CUDA(cudaMemcpyAsync(dox, ox.data(), sizeof(int) * ox.size(), cudaMemcpyHostToDevice, c.s));
+  GISSPA_CUDA(cudaMemcpyAsync(doy, oy.data(), sizeof(int) * oy.size(), cudaMemcpyHostToDevice, c.s));
+  float2* w = buf<float2>(h->win_c, (size_t)W * c.L2);
+  float2* tmp = buf<float2>(h->win_tmp, (size_t)W * c.L2);
+  gather_windows(img, nx, ny, dox, doy, bx, W, l, w, c.s);
+  h->fft.fft2(w, tmp, W, l, l, -1, 1.0f / (float)c.L2, c.s);
+  rms_normalise(w, W, l, nullptr, c.s);
+  h->fft.transpose(w, buf<float2>(h->ispec, (size_t)W * (l / 2 + 1) * l), W, l, l, c.s, l / 2 + 1);
+}
+
+// RotateTemplate (norm.cu:479-521): rotate, mask, (x - mean)/sqrt(var), FFT / l^2.
+void template_spectra_at(Ctx& c, float theta) {
+  gisspa_handle* h = c.h;
+  const int l = c.l, nt = h->nt, hs = l / 2 + 1;
+  const double rad = (double)theta * kRefPi / 180.0;
+  float2* rot = buf<float2>(h->rot, (size_t)nt * c.L2);
+  float2* rtmp = buf<float2>(h->rot_tmp, (size_t)nt * hs * l);
+  double* sums = buf<double>(h->rsums, 2 * (size_t)nt);
+  rotate_batch(h->prep_real.as<float>(), nt, l, (float)std::cos(rad), (float)std::sin(rad), true, h->cfg.diameter,
+               h->cfg.edge_half_width, rot, sums, c.s);
+  h->fft.rows(rot, (long long)nt * l, l, -1, 1.f, c.s);
+  h->fft.transpose(rot, rtmp, nt, l, l, c.s, hs);
+  h->fft.rows(rtmp, (long long)nt * hs, l, -1, 1.f, c.s);
+  void* ts = h->tspec.ensure(spec_bytes(h->cfg.spectrum_precision) * (size_t)nt * hs * l);
+  finalize_spectra(rtmp, nt, l, sums, h->cfg.spectrum_precision, ts, 1.0 / (double)c.L2, c.s);
+}
+
+void choose_batches(const gisspa_config& cfg, int l, int W, int nt, int& D, int& E) {
+  const long long per_pair = (long long)(l / 2) * l * (long long)sizeof(float2);
+  const long long budget = 96LL << 20;
+  E = cfg.window_batch > 0 ? cfg.window_batch : (l >= 1024 ? 4 : 8);
+  E = std::max(1, std::min(E, W));
+  D = cfg.template_batch > 0 ? cfg.template_batch : (int)std::max(1LL, budget / per_pair / E);
+  D = std::max(1, std::min(D, nt));
+}
+
+// One correlation sweep at one angle over every (window, template) pair.
+long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, int nt, CorrArgs args, int D, int E) {
+  gisspa_handle* h = c.h;
+  const int l = c.l;
+  float2* Q = buf<float2>(h->Q, (size_t)D * E * (l / 2) * l);
+  const float2* twL = h->fft.twiddles(l);
+  const float2* twNZ = h->fft.twiddles(l / 2);
+  long long pairs = 0;
+  for (int n0 = 0; n0 < nt; n0 += D) {
+    const int d = std::min(D, nt - n0);
+    for (int b0 = 0; b0 < W; b0 += E) {
+      const int e = std::min(E, W - b0);
+      CorrLaunch cl{l, e, d, h->cfg.spectrum_precision, epi};
+      if (epi == EPI_NONORM) cl.spec = h->cfg.spectrum_precision;
+      args.Q = Q;
+      args.b0 = b0;
+      args.n0 = n0;
+      args.D = d;
+      cudaEvent_t* ev = nullptr;
+      if ((h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples) {
+        ev = h->sev[h->n_samples];
+        h->sample_pairs[h->n_samples] = d * e;
+        h->sample_d[h->n_samples] = d;
+        ++h->n_samples;
+      }
+      correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s, ev);
+      pairs += (long long)d * e;
+    }
+  }
+  return pairs;
+}
+
+void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_pick>& out) {
+  gisspa_handle* h = c.h;
+  const gisspa_config& cfg = h->cfg;
+  const int l = c.l, nt = h->nt;
+  const long long N = (long long)nx * ny;
+  GISSPA_CUDA(cudaEventRecord(h->ev[0], c.s));
+  prepare_templates(c);
+  // micrograph
+  float* stats = buf<float>(h->stats, 4);
+  double* scr = buf<double>(h->scratch, 16);
+  image_stats(d_img, nx, ny, (cfg.quirks & GISSPA_QUIRK_OUTLIER_FP32_SERIAL) != 0, stats, scr, c.s);
+  float2* G = buf<float2>(h->img_c, N);
+  image_load(d_img, N, stats, true, cfg.invert != 0, G, c.s);
+  preprocess_full(c, G, nx, ny, true);
+  float* img = buf<float>(h->img_pre, N);
+  real_part(G, img, N, 1.f, c.s);
+  const std::vector<int> ox = window_offsets(nx, l, cfg.overlap), oy = window_offsets(ny, l, cfg.overlap);
+  const int bx = (int)ox.size(), W = bx * (int)oy.size();
+  window_spectra(c, img, nx, ny, ox, oy);
+  GISSPA_CUDA(cudaEventRecord(h->ev[1], c.s));
+
+  const std::vector<float> angles = angle_list(cfg.phistep);
+  const int n_euler = (cfg.quirks & GISSPA_QUIRK_NEULER_TRUNC) ? (int)(360.0f / cfg.phistep) : (int)angles.size();
+  const int batch = (cfg.quirks & GISSPA_QUIRK_COUNT_PADDED_TEMPLATES) ? std::max(nt, W) : nt;
+  const double Ntot = (double)batch * n_euler;
+  const bool topk = cfg.pick_mode == GISSPA_PICK_TOPK;
+  const size_t npix = (size_t)W * c.L2;
+  double* S1 = buf<double>(h->S1, npix);
+  double* S2 = buf<double>(h->S2, npix);
+  GISSPA_CUDA(cudaMemsetAsync(S1, 0, sizeof(double) * npix, c.s));
+  GISSPA_CUDA(cudaMemsetAsync(S2, 0, sizeof(double) * npix, c.s));
+  CorrArgs args{};
+  args.S1 = S1;
+  args.S2 = S2;
+  args.nt_real = nt;
+  args.nt_total = nt;
+  args.offx = h->offx.as<int>();
+  args.offy = h->offy.as<int>();
+  args.bx = bx;
+  args.nx = nx;
+  args.ny = ny;
+  args.dmin = cfg.diameter;
+  args.thresh = cfg.threshold;
+  if (topk) {
+    args.cmax = buf<float>(h->cmax, npix);
+    args.carg = buf<int>(h->carg, npix);
+    fill_kernel<<<ceil_div((long long)npix, 256), 256, 0, c.s>>>(args.cmax, args.carg, (long long)npix);
+    GISSPA_LAUNCH_CHECK();
+  }
+  int D, E;
+  choose_batches(cfg, l, W, nt, D, E);
+  const void* T = nullptr;
+  long long pairs = 0;
+  // sweep 1 (ComputeCCGSum norm.cu:523-544), or the single top-K sweep
+  for (size_t a = 0; a < angles.size(); ++a) {
+    template_spectra_at(c, angles[a]);
+    T = h->tspec.as<void>();
+    args.angle = (int)a;
+    pairs += correlate_all(c, topk ? EPI_TOPK : EPI_SUM, h->ispec.as<float2>(), W, T, nt, args, D, E);
+  }
+  float2* ms = buf<float2>(h->musig, npix);
+  musig_kernel<<<ceil_div((long long)npix, 256), 256, 0, c.s>>>(S1, S2, (long long)npix, Ntot, ms);
+  GISSPA_LAUNCH_CHECK();
+  GISSPA_CUDA(cudaEventRecord(h->ev[2], c.s));
+  args.musig = ms;
+
+  if (!topk) {
+    // sweep 2 (PickParticles norm.cu:554-600)
+    unsigned cap = (unsigned)std::max<size_t>(h->cand.size() / sizeof(Cand), 1u << 16);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      Cand* cand = buf<Cand>(h->cand, cap);
+      unsigned* cnt = buf<unsigned>(h->cand_count, 1);
+      GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
+      args.cand = cand;
+      args.cand_count = cnt;
+      args.cand_cap = cap;
+      for (size_t a = 0; a < angles.size(); ++a) {
+        template_spectra_at(c, angles[a]);
+        args.angle = (int)a;
+        pairs += correlate_all(c, EPI_CHUNK, h->ispec.as<float2>(), W, h->tspec.as<void>(), nt, args, D, E);
+      }
+      GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
+      unsigned count = 0;
+      GISSPA_CUDA(cudaMemcpyAsync(&count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c.s));
+      GISSPA_CUDA(cudaStreamSynchronize(c.s));
+      h->st.candidates = count;
+      if (count > cap) {  // grow and repeat the second sweep only
+        cap = count + count / 4 + 1024;
+        continue;
+      }
+      std::vector<Cand> hc(count);
+      if (count)
+        GISSPA_CUDA(cudaMemcpyAsync(hc.data(), cand, sizeof(Cand) * count, cudaMemcpyDeviceToHost, c.s));
+      GISSPA_CUDA(cudaStreamSynchronize(c.s));
+      // reference output order: angle, window (j outer, i inner), template, chunk (norm.cu:561-598)
+      std::sort(hc.begin(), hc.end(), [](const Cand& u, const Cand& v) {
+        if (u.angle != v.angle) return u.angle < v.angle;
+        if (u.window != v.window) return u.window < v.window;
+        if (u.templ != v.templ) return u.templ < v.templ;
+        return u.chunk < v.chunk;
+      });
+      out.reserve(hc.size());
+      for (const Cand& cd : hc) {
+        gisspa_pick pk{};
+        pk.score = cd.score;
+        pk.x = (float)(ox[cd.window % bx] + cd.x);
+        pk.y = (float)(oy[cd.window / bx] + cd.y);
+        float cur_e = 360.0f - angles[cd.angle];  // norm.cu:700-701
+        if (cur_e >= 360.0f) cur_e -= 360.0f;
+        pk.angle = cur_e;
+        pk.theta = angles[cd.angle];
+        pk.template_id = cd.templ;
+        pk.window = cd.window;
+        pk.tile = 0;
+        pk.angle_index = cd.angle;
+        pk.chunk = cd.chunk;
+        out.push_back(pk);
+      }
+      break;
+    }
+  } else {
+    unsigned long long* zk = buf<unsigned long long>(h->zkey, N);
+    GISSPA_CUDA(cudaMemsetAsync(zk, 0, sizeof(unsigned long long) * N, c.s));
+    zmap_kernel<<<dim3(ceil_div(c.L2, 256), W), 256, 0, c.s>>>(args.cmax, args.carg, ms, l, args.offx, args.offy, bx,
+                                                                nx, ny, zk);
+    GISSPA_LAUNCH_CHECK();
+    unsigned cap = (unsigned)std::max<size_t>(h->zcand.size() / sizeof(ZCand), 1u << 16);
+    std::vector<ZCand> hz;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      ZCand* zc = buf<ZCand>(h->zcand, cap);
+      unsigned* cnt = buf<unsigned>(h->zcount, 1);
+      GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
+      zcompact_kernel<<<ceil_div(N, 256), 256, 0, c.s>>>(zk, nx, ny, cfg.threshold, cfg.diameter, args.carg, l,
+                                                          args.offx, args.offy, bx, zc, cnt, cap);
+      GISSPA_LAUNCH_CHECK();
+      unsigned count = 0;
+      GISSPA_CUDA(cudaMemcpyAsync(&count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c.s));
+      GISSPA_CUDA(cudaStreamSynchronize(c.s));
+      if (count > cap) {
+        cap = count + 1024;
+        continue;
+      }
+      hz.resize(count);
+      if (count) GISSPA_CUDA(cudaMemcpy(hz.data(), zc, sizeof(ZCand) * count, cudaMemcpyDeviceToHost));
+      break;
+    }
+    GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
+    h->st.candidates = (long long)hz.size();
+    std::sort(hz.begin(), hz.end(), [](const ZCand& u, const ZCand& v) {
+      if (u.z != v.z) return u.z > v.z;
+      return u.q < v.q;
+    });
+    const double r2 = (double)cfg.exclusion_radius * cfg.exclusion_radius;
+    std::vector<int> acc;
+    for (const ZCand& zc : hz) {
+      if ((int)acc.size() >= cfg.topk) break;
+      const int x = zc.q % nx, y = zc.q / nx;
+      bool ok = true;
+      for (int q2 : acc) {
+        const double dx = x - q2 % nx, dy = y - q2 / nx;
+        if (dx * dx + dy * dy <= r2) {
+          ok = false;
+          break;
+        }
+      }
+      if (!ok) continue;
+      acc.push_back(zc.q);
+      gisspa_pick pk{};
+      pk.score = zc.z;
+      pk.x = (float)x;
+      pk.y = (float)y;
+      const int a = zc.arg / nt, n = zc.arg % nt;
+      float cur_e = 360.0f - angles[a];
+      if (cur_e >= 360.0f) cur_e -= 360.0f;
+      pk.angle = cur_e;
+      pk.theta = angles[a];
+      pk.template_id = n;
+      pk.window = zc.win;
+      pk.angle_index = a;
+      pk.chunk = (int)acc.size() - 1;
+      out.push_back(pk);
+    }
+  }
+  h->st.pairs = pairs;
+}
+
+// norm_type = 0 (SearchNoNorm, nonorm.cu): 720^2 tiles, rotate the windows, per-template best.
+void search_nonorm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_pick>& out) {
+  gisspa_handle* h = c.h;
+  const gisspa_config& cfg = h->cfg;
+  const int l = c.l, nt = h->nt, ts = cfg.tile_size, hs = l / 2 + 1;
+  GISSPA_CUDA(cudaEventRecord(h->ev[0], c.s));
+  prepare_templates(c);
+  // tiles (TileImages, tileimages.cpp:18-70): column-major, centres clamped to the image
+  const int cols = (int)std::ceil((double)nx / ts), rows = (int)std::ceil((double)ny / ts);
+  const int x_step = nx / cols, y_step = ny / rows;
+  std::vector<int> tx, ty;
+  for (int j = 0; j < cols; ++j) {
+    const int cxx = j == 0 ? ts / 2 : (j == cols - 1 ? nx - ts / 2 : x_step * (2 * j + 1) / 2);
+    for (int i = 0; i < rows; ++i) {
+      const int cyy = i == 0 ? ts / 2 : (i == rows - 1 ? ny - ts / 2 : y_step * (2 * i + 1) / 2);
+      tx.push_back(std::max(cxx - ts / 2, 0));
+      ty.push_back(std::max(cyy - ts / 2, 0));
+    }
+  }
+  const int bx = window_count_nonorm(ts, l, cfg.overlap), W = bx * bx;
+  std::vector<int> woff(bx);
+  for (int k = 0; k < bx; ++k) woff[k] = k * (l - cfg.overlap);  // split_IMG unclamped (kernels.cu:605-624)
+  const std::vector<float> angles = angle_list(cfg.phistep);
+  int D, E;
+  choose_batches(cfg, l, W, nt, D, E);
+  const long long TS2 = (long long)ts * ts;
+  int* dtx = buf<int>(h->offx, std::max<size_t>(woff.size(), 2));
+  int* dty = buf<int>(h->offy, std::max<size_t>(woff.size(), 2));
+  unsigned long long* nk = buf<unsigned long long>(h->nn_key, (size_t)W * nt);
+  double* nsum = buf<double>(h->nn_sum, (size_t)W * nt * 2);
+  std::vector<unsigned long long> hk((size_t)W * nt);
+  std::vector<double> hsum((size_t)W * nt * 2);
+  long long pairs = 0;
+  GISSPA_CUDA(cudaEventRecord(h->ev[1], c.s));
+  for (size_t t = 0; t < tx.size(); ++t) {
+    // LoadImage (nonorm.cu:157-165): the tile, inverted on request
+    int tile_off[2] = {tx[t], ty[t]};
+    GISSPA_CUDA(cudaMemcpyAsync(dtx, &tile_off[0], sizeof(int), cudaMemcpyHostToDevice, c.s));
+    GISSPA_CUDA(cudaMemcpyAsync(dty, &tile_off[1], sizeof(int), cudaMemcpyHostToDevice, c.s));
+    float2* G = buf<float2>(h->img_c, TS2);
+    gather_windows(d_img, nx, ny, dtx, dty, 1, 1, ts, G, c.s);
+    float* tile = buf<float>(h->tile_real, TS2);
+    if (cfg.phase_flip == 1) {  // PreprocessImage (nonorm.cu:346-389), no DC zeroing
+      if (cfg.invert) {
+        real_part(G, tile, TS2, -1.f, c.s);
+        to_complex(tile, G, TS2, c.s);
+      }
+      preprocess_full(c, G, ts, ts, false);
+    }
+    real_part(G, tile, TS2, (cfg.invert && cfg.phase_flip != 1) ? -1.f : 1.f, c.s);
+    // SplitImage (nonorm.cu:391-450)
+    GISSPA_CUDA(cudaMemcpyAsync(dtx, woff.data(), sizeof(int) * bx, cudaMemcpyHostToDevice, c.s));
+    GISSPA_CUDA(cudaMemcpyAsync(dty, woff.data(), sizeof(int) * bx, cudaMemcpyHostToDevice, c.s));
+    float2* w = buf<float2>(h->win_c, (size_t)W * c.L2);
+    float2* wtmp = buf<float2>(h->win_tmp, (size_t)W * c.L2);
+    gather_windows(tile, ts, ts, dtx, dty, bx, W, l, w, c.s);
+    if (cfg.phase_flip == 1) {
+      h->fft.fft2(w, wtmp, W, l, l, -1, 1.0f / (float)c.L2, c.s);
+      rms_normalise(w, W, l, nullptr, c.s);
+      h->fft.fft2(w, wtmp, W, l, l, +1, 1.f, c.s);
+    }
+    float* wr = buf<float>(h->win_real, (size_t)W * c.L2);
+    real_part(w, wr, (long long)W * c.L2, 1.f, c.s);
+    for (size_t a = 0; a < angles.size(); ++a) {
+      const float e = angles[a];
+      const double rad = (double)e * kRefPi / 180.0;
+      // PickParticles (nonorm.cu:452-537): rotate the windows, transform, correlate
+      float2* rot = buf<float2>(h->rot, (size_t)W * c.L2);
+      float2* rtmp = buf<float2>(h->rot_tmp, (size_t)W * hs * l);
+      rotate_batch(wr, W, l, (float)std::cos(rad), (float)std::sin(rad), false, 0.f, 0.f, rot, nullptr, c.s);
+      h->fft.rows(rot, (long long)W * l, l, -1, 1.f, c.s);
+      h->fft.transpose(rot, rtmp, W, l, l, c.s, hs);
+      h->fft.rows(rtmp, (long long)W * hs, l, -1, 1.f, c.s);
+      float2* I = buf<float2>(h->ispec, (size_t)W * hs * l);
+      finalize_spectra(rtmp, W, l, nullptr, GISSPA_SPEC_FP32, I, 1.0 / (double)c.L2, c.s);
+      GISSPA_CUDA(cudaMemsetAsync(nk, 0, sizeof(unsigned long long) * W * nt, c.s));
+      GISSPA_CUDA(cudaMemsetAsync(nsum, 0, sizeof(double) * W * nt * 2, c.s));
+      CorrArgs args{};
+      args.nt_real = nt;
+      args.nt_total = nt;
+      args.angle = (int)a;
+      args.nn_key = nk;
+      args.nn_sum = nsum;
+      args.border = cfg.diameter / 4;
+      pairs += correlate_all(c, EPI_NONORM, I, W, h->tspec.as<void>(), nt, args, D, E);
+      GISSPA_CUDA(cudaMemcpyAsync(hk.data(), nk, sizeof(unsigned long long) * W * nt, cudaMemcpyDeviceToHost, c.s));
+      GISSPA_CUDA(cudaMemcpyAsync(hsum.data(), nsum, sizeof(double) * W * nt * 2, cudaMemcpyDeviceToHost, c.s));
+      GISSPA_CUDA(cudaStreamSynchronize(c.s));
+      // host merge (nonorm.cu:498-534): best window per template, centre rotated back
+      std::vector<float> bs(nt, 0.f), bxp(nt, 0.f), byp(nt, 0.f);
+      const double ce = std::cos(rad), se = std::sin(rad);
+      for (int b = 0; b < W; ++b) {
+        const int i = b % bx, j = b / bx;
+        for (int n = 0; n < nt; ++n) {
+          const unsigned long long k = hk[(size_t)b * nt + n];
+          double peak = 0, pos = 0;
+          if (k) {
+            uint32_t hi = (uint32_t)(k >> 32);
+            uint32_t bits = (hi & 0x80000000u) ? (hi & 0x7fffffffu) : ~hi;
+            float pv;
+            std::memcpy(&pv, &bits, 4);
+            const unsigned lo = (unsigned)(k & 0xFFFFFFFFu);
+            const int chunk = (int)(0xFFFFFu - (lo >> 8));
+            peak = pv;
+            pos = (double)(chunk * 256 + (int)(lo & 0xFFu));
+          }
+          const double s1 = hsum[2 * ((size_t)b * nt + n)], s2 = hsum[2 * ((size_t)b * nt + n) + 1];
+          const double rA = s1 - peak, rB = s2 - peak * peak, rC = (double)c.L2 - 1;
+          const double sd = std::sqrt(rB / rC - (rA / rC) * (rA / rC));
+          const double score = sd == 0 ? 0.0 : peak / sd;
+          const int cx = (int)pos % l, cy = (int)pos / l;
+          const double centerx = i * (l - cfg.overlap) + (cx - l / 2) * ce + (cy - l / 2) * se + l / 2;
+          const double centery = j * (l - cfg.overlap) + (cy - l / 2) * ce - (cx - l / 2) * se + l / 2;
+          if (bs[n] < (float)score && centerx >= 0 && centerx < ts && centery >= 0 && centery < ts) {
+            bs[n] = (float)score;
+            bxp[n] = (float)centerx;
+            byp[n] = (float)centery;
+          }
+        }
+      }
+      for (int n = 0; n < nt; ++n)  // OutputScore (nonorm.cu:539-557)
+        if (bs[n] >= cfg.threshold) {
+          gisspa_pick pk{};
+          pk.score = bs[n];
+          pk.x = bxp[n];
+          pk.y = byp[n];
+          pk.angle = e;
+          pk.theta = e;
+          pk.template_id = n;
+          pk.window = -1;
+          pk.tile = (int)t;
+          pk.angle_index = (int)a;
+          pk.chunk = -1;
+          out.push_back(pk);
+        }
+    }
+  }
+  GISSPA_CUDA(cudaEventRecord(h->ev[2], c.s));
+  GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
+  h->st.pairs = pairs;
+}
+
+}  // namespace
+
+void debug_stage(gisspa_handle* h, int what, const float* d_img, int nx, int ny, const gisspa_ctf& ctf, float theta,
+                 void* out, size_t bytes) {
+  Ctx c{h, h->stream, h->cfg.window_size, (long long)h->cfg.window_size * h->cfg.window_size,
+        make_params(h->cfg, ctf)};
+  const gisspa_config& cfg = h->cfg;
+  const int l = c.l, hs = l / 2 + 1;
+  auto fetch = [&](const void* src, size_t need) {
+    if (bytes < need) throw CudaError{cudaErrorInvalidValue, "debug_stage: output buffer too small"};
+    GISSPA_CUDA(cudaMemcpyAsync(out, src, need, cudaMemcpyDeviceToHost, c.s));
+    GISSPA_CUDA(cudaStreamSynchronize(c.s));
+  };
+  if (what == GISSPA_STAGE_MUSIG) {
+    if (!h->musig.size() || cfg.norm_type == 0)
+      throw CudaError{cudaErrorInvalidValue, "debug_stage: no norm_type=1 search has run"};
+    fetch(h->musig.as<void>(), std::min(bytes, h->musig.size()));
+    return;
+  }
+  if (what == GISSPA_STAGE_TEMPLATE_SPECTRA && cfg.norm_type == 0)
+    throw CudaError{cudaErrorInvalidValue, "debug_stage: per-angle template spectra exist for norm_type=1 only"};
+  prepare_templates(c);
+  if (what == GISSPA_STAGE_TEMPLATES) {
+    if (cfg.norm_type != 0) {
+      fetch(h->prep_real.as<void>(), sizeof(float) * (size_t)h->nt * c.L2);
+    } else {
+      float2* tmp = buf<float2>(h->tb_tmp, (size_t)h->nt * hs * l);
+      h->fft.transpose(h->tb.as<float2>(), tmp, h->nt, l, l, c.s, hs);
+      fetch(tmp, sizeof(float2) * (size_t)h->nt * hs * l);
+    }
+    return;
+  }
+  if (what == GISSPA_STAGE_TEMPLATE_SPECTRA) {
+    template_spectra_at(c, theta);
+    float2* tmp = buf<float2>(h->tb_tmp, (size_t)h->nt * hs * l);
+    finalize_spectra(h->rot_tmp.as<float2>(), h->nt, l, h->rsums.as<double>(), GISSPA_SPEC_FP32, tmp,
+                     1.0 / (double)c.L2, c.s);
+    fetch(tmp, sizeof(float2) * (size_t)h->nt * hs * l);
+    return;
+  }
+  if (!d_img) throw CudaError{cudaErrorInvalidValue, "debug_stage: image required"};
+  const long long N = (long long)nx * ny;
+  float* stats = buf<float>(h->stats, 4);
+  double* scr = buf<double>(h->scratch, 16);
+  image_stats(d_img, nx, ny, (cfg.quirks & GISSPA_QUIRK_OUTLIER_FP32_SERIAL) != 0, stats, scr, c.s);
+  float2* G = buf<float2>(h->img_c, N);
+  image_load(d_img, N, stats, true, cfg.invert != 0, G, c.s);
+  preprocess_full(c, G, nx, ny, true);
+  float* img = buf<float>(h->img_pre, N);
+  real_part(G, img, N, 1.f, c.s);
+  if (what == GISSPA_STAGE_IMAGE) {
+    fetch(img, sizeof(float) * N);
+    return;
+  }
+  const std::vector<int> ox = window_offsets(nx, l, cfg.overlap), oy = window_offsets(ny, l, cfg.overlap);
+  window_spectra(c, img, nx, ny, ox, oy);
+  if (what == GISSPA_STAGE_WINDOW_SPECTRA) {
+    fetch(h->ispec.as<void>(), sizeof(float2) * ox.size() * oy.size() * hs * l);
+    return;
+  }
+  throw CudaError{cudaErrorInvalidValue, "debug_stage: unknown stage"};
+}
+
+void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int ntm, int spec, float* d_out) {
+  Ctx c{h, h->stream, h->cfg.window_size, (long long)h->cfg.window_size * h->cfg.window_size, DevParams{}};
+  const int l = c.l;
+  CorrArgs args{};
+  args.map_out = d_out;
+  args.nt_real = ntm;
+  args.nt_total = ntm;
+  float2* Q = buf<float2>(h->Q, (size_t)ntm * (l / 2) * l);
+  const float2* twL = h->fft.twiddles(l);
+  const float2* twNZ = h->fft.twiddles(l / 2);
+  // one launch per window: pair p = d covers template d of window b, written at [b][d]
+  for (int b = 0; b < nw; ++b) {
+    CorrLaunch cl{l, 1, ntm, spec, EPI_MAP};
+    args.Q = Q;
+    args.b0 = b;
+    args.n0 = 0;
+    args.D = ntm;
+    args.map_out = d_out + (size_t)b * ntm * c.L2;
+    correlate_launch(cl, static_cast<const float2*>(d_win), d_t, Q, args, twL, twNZ, c.s);
+  }
+  GISSPA_CUDA(cudaStreamSynchronize(c.s));
+}
+
+void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const gisspa_ctf& ctf,
+                std::vector<gisspa_pick>& out) {
+  Ctx c{h, h->stream, h->cfg.window_size, (long long)h->cfg.window_size * h->cfg.window_size,
+        make_params(h->cfg, ctf)};
+  const long long l0 = launch_counter();
+  h->st = gisspa_stats{};
+  h->n_samples = 0;
+  h->launch_index = 0;
+  if (h->cfg.norm_type != 0)
+    search_norm(c, d_img, nx, ny, out);
+  else
+    search_nonorm(c, d_img, nx, ny, out);
+  GISSPA_CUDA(cudaEventRecord(h->ev[4], c.s));
+  GISSPA_CUDA(cudaStreamSynchronize(c.s));
+  float ms = 0;
+  GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[0], h->ev[4]));
+  h->st.ms_total = ms;
+  GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[0], h->ev[1]));
+  h->st.ms_prep = ms;
+  GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]));
+  h->st.ms_sweep1 = ms;
+  GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[2], h->ev[3]));
+  h->st.ms_sweep2 = ms;
+  GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[3], h->ev[4]));
+  h->st.ms_pick = ms;
+  h->st.kernel_launches = launch_counter() - l0;
+  h->st.window_size = c.l;
+  double ta = 0, tb = 0, pp = 0, dd = 0;
+  for (int i = 0; i < h->n_samples; ++i) {
+    float a = 0, b = 0;
+    GISSPA_CUDA(cudaEventElapsedTime(&a, h->sev[i][0], h->sev[i][1]));
+    GISSPA_CUDA(cudaEventElapsedTime(&b, h->sev[i][1], h->sev[i][2]));
+    ta += a;
+    tb += b;
+    pp += h->sample_pairs[i];
+    dd += h->sample_d[i];
+  }
+  if (h->n_samples) {
+    h->st.pass_a_us = 1000.0 * ta / h->n_samples;
+    h->st.pass_b_us = 1000.0 * tb / h->n_samples;
+    h->st.pairs_per_launch = pp / h->n_samples;
+    h->st.templates_per_launch = dd / h->n_samples;
+  }
+  h->st.pass_samples = h->n_samples;
+}
+
+int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx, const int* ny,
+              const gisspa_ctf* ctfs, gisspa_pick* picks, size_t cap, size_t* offsets) {
+  std::vector<gisspa_pick> all, one;
+  offsets[0] = 0;
+  gisspa_stats total{};
+  for (int i = 0; i < n; ++i) {
+    one.clear();
+    int st = guarded(h, [&] {
+      GISSPA_CUDA(cudaSetDevice(h->device));
+      const size_t bytes = sizeof(float) * (size_t)nx[i] * ny[i];
+      h->img_in.ensure(bytes);
+      GISSPA_CUDA(cudaMemcpyAsync(h->img_in.as<float>(), images[i], bytes, cudaMemcpyHostToDevice, h->stream));
+      run_search(h, h->img_in.as<float>(), nx[i], ny[i], ctfs[i], one);
+    });
+    if (st) return st;
+    total.ms_total += h->st.ms_total;
+    total.ms_prep += h->st.ms_prep;
+    total.ms_sweep1 += h->st.ms_sweep1;
+    total.ms_sweep2 += h->st.ms_sweep2;
+    total.ms_pick += h->st.ms_pick;
+    total.pairs += h->st.pairs;
+    total.kernel_launches += h->st.kernel_launches;
+    total.candidates += h->st.candidates;
+    total.pass_a_us += h->st.pass_a_us / n;
+    total.pass_b_us += h->st.pass_b_us / n;
+    total.pairs_per_launch += h->st.pairs_per_launch / n;
+    total.templates_per_launch += h->st.templates_per_launch / n;
+    total.pass_samples += h->st.pass_samples;
+    total.window_size = h->st.window_size;
+    all.insert(all.end(), one.begin(), one.end());
+    offsets[i + 1] = all.size();
+  }
+  h->st = total;
+  if (all.size() > cap) {
+    h->err = "search_batch: " + std::to_string(all.size()) + " picks exceed capacity " + std::to_string(cap);
+    return GISSPA_ERR_CAPACITY;
+  }
+  if (!all.empty()) std::memcpy(picks, all.data(), sizeof(gisspa_pick) * all.size());
+  return GISSPA_OK;
+}
+
+}  // namespace gisspa

@@ -1,0 +1,96 @@
+// search.cuh — the search handle and the per-micrograph orchestration.
+#pragma once
+
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gisspa.h"
+#include "common.cuh"
+#include "fft_generic.cuh"
+
+struct gisspa_handle {
+  gisspa_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  std::string err;
+  gisspa::FftEngine fft;
+
+  // template stack (device copy of the caller's array)
+  gisspa::DevBuf d_stack;
+  int nt = 0, tw = 0, th = 0;
+  bool templates_ready = false;
+
+  // template preparation
+  gisspa::DevBuf tb, tb_tmp, prep_real, table, tspec;
+  // per-angle rotation
+  gisspa::DevBuf rot, rot_tmp, rsums;
+  // micrograph and windows
+  gisspa::DevBuf img_in, img_c, img_tmp, img_pre, tile_real;
+  gisspa::DevBuf win_c, win_tmp, win_real, ispec;
+  gisspa::DevBuf offx, offy;
+  // shells, statistics
+  gisspa::DevBuf ra, rb, stats, scratch;
+  // per-window-pixel state
+  gisspa::DevBuf S1, S2, cmax, carg, musig;
+  // correlation intermediate and outputs
+  gisspa::DevBuf Q, cand, cand_count, nn_key, nn_sum, zkey, zcand, zcount;
+
+  gisspa_stats st{};
+  // sampled per-launch timing of the correlation kernels
+  static constexpr int kSamples = 64;
+  cudaEvent_t sev[kSamples][3] = {};
+  int sample_pairs[kSamples] = {}, sample_d[kSamples] = {};
+  int n_samples = 0;
+  long long launch_index = 0;
+
+  ~gisspa_handle() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& r : sev)
+      for (auto& e : r)
+        if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace gisspa {
+
+// Shape / parameter checks (the reference has none; norm.cu:222-224 needs l^2 % 256 == 0).
+int validate_config(const gisspa_config& c, std::string& err);
+int validate_image(const gisspa_config& c, int nx, int ny, std::string& err);
+
+// Runs fn, turning CUDA and allocation failures into status codes + h->err.
+template <typename F>
+int guarded(gisspa_handle* h, F&& fn) {
+  try {
+    fn();
+    return GISSPA_OK;
+  } catch (const CudaError& e) {
+    h->err = std::string(cudaGetErrorString(e.code)) + " at " + e.where;
+    cudaGetLastError();
+    return e.code == cudaErrorMemoryAllocation ? GISSPA_ERR_NOMEM : GISSPA_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    h->err = "out of host memory";
+    return GISSPA_ERR_NOMEM;
+  }
+}
+
+void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const gisspa_ctf& ctf,
+                std::vector<gisspa_pick>& out);
+int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx, const int* ny,
+              const gisspa_ctf* ctfs, gisspa_pick* picks, size_t cap, size_t* offsets);
+
+void debug_stage(gisspa_handle* h, int what, const float* d_img, int nx, int ny, const gisspa_ctf& ctf, float theta,
+                 void* out, size_t bytes);
+void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int ntm, int spec, float* d_out);
+
+// Window offsets along one axis (blocks_one_axis, norm.cu:68-81).
+std::vector<int> window_offsets(int len, int l, int ov);
+// Window count along one axis for norm_type=0 (nonorm.cu:71-81).
+int window_count_nonorm(int len, int l, int ov);
+// Float-stepped angle sequence: for (float e = 0; e < 360; e += step) (norm.cu:684).
+std::vector<float> angle_list(float step);
+
+}  // namespace gisspa

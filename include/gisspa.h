@@ -1,0 +1,202 @@
+/*
+ * gisspa.h — C-ABI of the B200 template-matching search library (libgisspa.so).
+ *
+ * This is the drop-in boundary for GisSPA's per-micrograph search loop.  Each
+ * entry point names the reference interface it replaces (paths are relative to
+ * the GisSPA_v2.0 source tree).  All pointers are plain host pointers unless the
+ * name says "device"; no CUDA or C++ types cross the boundary.  Every call
+ * returns an int status (GISSPA_OK == 0) and never exits the process; the text
+ * of the last error is available from gisspa_last_error().
+ *
+ * Threading: one handle per device.  Calls on one handle are not thread-safe;
+ * separate handles are independent.  Each call makes the handle's device
+ * current itself (the reference relies on cudaSetDevice in the constructor,
+ * norm.cu:64).
+ */
+#ifndef GISSPA_H
+#define GISSPA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference has none: it calls exit(-1), utils.h:24-38) ---- */
+enum {
+  GISSPA_OK = 0,
+  GISSPA_ERR_ARG = 1,         /* null pointer or out-of-range argument */
+  GISSPA_ERR_SHAPE = 2,       /* window_size % 16 != 0, window larger than image, ... */
+  GISSPA_ERR_UNSUPPORTED = 3, /* accepted by the reference but not by this build */
+  GISSPA_ERR_CUDA = 4,        /* CUDA runtime error (text in gisspa_last_error) */
+  GISSPA_ERR_NOMEM = 5,       /* device or host allocation failed */
+  GISSPA_ERR_CAPACITY = 6,    /* pick buffer too small: *n_out holds the count needed */
+  GISSPA_ERR_STATE = 7,       /* call order (search before set_templates, ...) */
+  GISSPA_ERR_TIMEOUT = 8,     /* a bounded device wait gave up */
+  GISSPA_ERR_IO = 9           /* file could not be read or parsed */
+};
+
+/* ---- pick modes ---- */
+enum {
+  GISSPA_PICK_CHUNK = 0, /* reference picks: two sweeps, one pick per 256-pixel chunk
+                            with z >= threshold (norm.cu:554-600) */
+  GISSPA_PICK_TOPK = 1   /* one sweep: per-pixel max z over templates x angles, then
+                            greedy top-K with an exclusion radius */
+};
+
+/* ---- template-spectrum storage precision (FFT arithmetic is FP32 in all cases) ---- */
+enum { GISSPA_SPEC_FP32 = 0, GISSPA_SPEC_FP16 = 1, GISSPA_SPEC_BF16 = 2 };
+
+/* ---- reference quirks (bit set = reproduce the reference's behaviour) ---- */
+/* LoadImage: mean/sigma by a serial FP32 sum, bounds truncated to int (norm.cu:157-171). */
+#define GISSPA_QUIRK_OUTLIER_FP32_SERIAL 0x1
+/* Templates beyond N_T (when windows outnumber templates) count in N (norm.cu:91, 550).
+   The reference reads past the template array there; this build uses all-zero maps. */
+#define GISSPA_QUIRK_COUNT_PADDED_TEMPLATES 0x2
+/* N_euler = (int)(360 / phistep) instead of the float-stepped loop count (norm.cu:550, 684). */
+#define GISSPA_QUIRK_NEULER_TRUNC 0x4
+#define GISSPA_QUIRKS_REFERENCE 0x7
+
+/* Search configuration.  The first block mirrors the reference Config keys
+ * (EMReader/DataReader2.h:19-44) and Parameters constants (DataReader2.h:73-77). */
+typedef struct gisspa_config {
+  float angpix, phistep, kk, energy, cs, highres, lowres, diameter, threshold;
+  int window_size, overlap, norm_type, invert, phase_flip;
+  float edge_half_width, ampconst, a, b, b2, bfactor, bfactor2, bfactor3;
+  /* additions (no counterpart in the reference) */
+  int pick_mode;          /* GISSPA_PICK_* */
+  int topk;               /* K for GISSPA_PICK_TOPK */
+  float exclusion_radius; /* pixels, GISSPA_PICK_TOPK */
+  int spectrum_precision; /* GISSPA_SPEC_* */
+  int template_batch;     /* templates per correlation pass (0 = automatic) */
+  int window_batch;       /* windows per correlation pass (0 = automatic) */
+  int quirks;             /* GISSPA_QUIRK_* bits */
+  int tile_size;          /* norm_type=0 tile edge; reference constant 720 (utils/constants.h:5) */
+} gisspa_config;
+
+/* Per-micrograph CTF, as in an LST line "defocus= dfdiff= dfang=" (DataReader2.h:93-103).
+   defocus and dfdiff in micrometres, dfang in degrees. */
+typedef struct gisspa_ctf {
+  double defocus, dfdiff, dfang;
+} gisspa_ctf;
+
+/* One pick.  x, y, angle and score are the values the reference prints in its
+ * pick-list line (norm.cu:602-618, nonorm.cu:539-557). */
+typedef struct gisspa_pick {
+  float score;
+  float x, y;      /* centre; tile-local for norm_type=0, as the reference prints it */
+  float angle;     /* printed in-plane angle: 360-theta for norm_type=1, theta for 0 */
+  int template_id; /* index into the template stack */
+  int window;      /* window index i + j*block_x */
+  int tile;        /* norm_type=0 tile index (column-major, tileimages.cpp:27-70), else 0 */
+  int angle_index; /* index of theta in the float-stepped angle sequence */
+  int chunk;       /* chunk pick: 256-pixel chunk within the window; top-K: rank */
+  float theta;     /* search angle theta in degrees (before the printed convention) */
+} gisspa_pick;
+
+/* Paths and run range of a reference config file (DataReader2.h:19-44). */
+typedef struct gisspa_run_paths {
+  char input[1024];
+  char template_path[1024];
+  char eulerfile[1024];
+  char output[1024];
+  int first, last, gpu_id;
+} gisspa_run_paths;
+
+/* Per-call timing and counters. */
+typedef struct gisspa_stats {
+  double ms_total, ms_prep, ms_sweep1, ms_sweep2, ms_pick;
+  long long pairs;            /* window x template x angle correlations evaluated */
+  long long kernel_launches;  /* launches of this library's kernels in the last search */
+  long long candidates;       /* picks found before the capacity check */
+  /* CUDA-event timing of a sample of correlation launches (every 16th launch pair) */
+  double pass_a_us, pass_b_us; /* mean duration of one pass A / pass B launch */
+  double pairs_per_launch;     /* mean (window, template) pairs per sampled launch */
+  double templates_per_launch; /* mean template batch depth D of the sampled launches */
+  int pass_samples;
+  int window_size;
+} gisspa_stats;
+
+typedef struct gisspa_handle gisspa_handle;
+
+/* Fill *cfg with the reference defaults (DataReader2.h:19-44, 73-77) plus the
+ * defaults of the additions. */
+void gisspa_config_default(gisspa_config* cfg);
+
+/* Parse a reference config file ("key = value" tokens, unknown keys ignored;
+ * DataReader2.cpp:6-28).  Replaces Config::Config(path).  paths may be NULL. */
+int gisspa_config_load(const char* path, gisspa_config* cfg, gisspa_run_paths* paths);
+
+/* Replaces SearchNorm::SearchNorm / SearchNoNorm::SearchNoNorm (norm.cu:48-123,
+ * nonorm.cu:50-122).  Buffers are sized lazily and reused across micrographs. */
+int gisspa_create(const gisspa_config* cfg, int device, gisspa_handle** out);
+
+/* Replaces Templates(path, count) + LoadTemplate (templates.cpp:11-31, norm.cu:132-154).
+ * stack: n images of width x height floats, row-major, copied by the call. */
+int gisspa_set_templates(gisspa_handle* h, const float* stack, int n, int width, int height);
+
+/* Replaces SearchNorm::work / SearchNoNorm::work (norm.cu:620-660, nonorm.cu:559-589)
+ * for one micrograph held in host memory (ny rows of nx floats; not modified).
+ * Picks are written in the reference's output order.  If more than cap picks
+ * are found, GISSPA_ERR_CAPACITY is returned and *n_out holds the count. */
+int gisspa_search(gisspa_handle* h, const float* image, int nx, int ny, const gisspa_ctf* ctf,
+                  gisspa_pick* picks, size_t cap, size_t* n_out);
+
+/* As gisspa_search, with the micrograph already in this handle's device memory. */
+int gisspa_search_device(gisspa_handle* h, const float* d_image, int nx, int ny,
+                         const gisspa_ctf* ctf, gisspa_pick* picks, size_t cap, size_t* n_out);
+
+/* Replaces the per-micrograph loop of main.cu:36-50: n micrographs of uneven size,
+ * each with its own CTF, searched in one call.  picks of micrograph i are
+ * picks[offsets[i] .. offsets[i+1]) (offsets has n+1 entries). */
+int gisspa_search_batch(gisspa_handle* h, int n, const float* const* images, const int* nx,
+                        const int* ny, const gisspa_ctf* ctfs, gisspa_pick* picks, size_t cap,
+                        size_t* offsets);
+
+/* Format one pick as the reference's pick-list line (norm.cu:610-614), including
+ * the trailing newline.  Returns the number of characters written (excluding NUL)
+ * or -1 when cap is too small. */
+int gisspa_format_pick(const gisspa_pick* p, int lst_index, const char* micrograph_path,
+                       const gisspa_ctf* ctf, float euler1, float euler2, char* buf, size_t cap);
+
+/* Timing and counters of the last search on this handle. */
+int gisspa_get_stats(const gisspa_handle* h, gisspa_stats* out);
+
+/* Text of the last error on this handle (or of the last failed create when h is NULL). */
+const char* gisspa_last_error(const gisspa_handle* h);
+
+/* Replaces ~SearchNorm / ~SearchNoNorm (norm.cu:125-130). */
+void gisspa_destroy(gisspa_handle* h);
+
+/* Library version string. */
+const char* gisspa_version(void);
+
+/* Correlation maps of every (window, template) pair of device-resident half spectra
+ * (compute_corner_CCG kernels.cu:645-678 + cufftExecC2C norm.cu:532-537, real part / L^2).
+ * d_windows: n_windows x (L/2+1) x L complex FP32, kx-major (S[kx][ky]);
+ * d_templates: n_templates x (L/2+1) x L complex in `spec` precision, same layout;
+ * d_out: n_windows x n_templates x L x L floats, zero lag at (L/2, L/2).
+ * L is the handle's window_size.  Uses handle-owned scratch memory (allocated on
+ * first use). */
+int gisspa_cc_maps(gisspa_handle* h, const void* d_windows, int n_windows, const void* d_templates, int n_templates,
+                   int spec, float* d_out);
+
+/* ---- diagnostics: stage outputs for parity tests (no counterpart in the reference) ---- */
+enum {
+  GISSPA_STAGE_TEMPLATES = 1,        /* norm_type=1: float [nt][L][L] real-space prepared templates;
+                                        norm_type=0: float2 [nt][L/2+1][L] prepared spectra (kx-major) */
+  GISSPA_STAGE_IMAGE = 2,            /* float [ny][nx] preprocessed micrograph (norm_type=1) */
+  GISSPA_STAGE_WINDOW_SPECTRA = 3,   /* float2 [W][L/2+1][L] normalised window spectra (kx-major) */
+  GISSPA_STAGE_TEMPLATE_SPECTRA = 4, /* float2 [nt][L/2+1][L] rotated template spectra at theta */
+  GISSPA_STAGE_MUSIG = 5             /* float2 [W][L][L] (mu, 1/sigma) of the last norm_type=1 search */
+};
+/* Runs the preparation stages for `image` (host, may be NULL for stages 1 and 5) and
+ * copies the requested stage output to host memory `out` of `bytes` bytes. */
+int gisspa_debug_stage(gisspa_handle* h, int what, const float* image, int nx, int ny, const gisspa_ctf* ctf,
+                       float theta, void* out, size_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GISSPA_H */

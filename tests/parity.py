@@ -1,0 +1,110 @@
+"""Shared helpers of the parity tests: small seeded cases and pick-list comparison."""
+from __future__ import annotations
+
+import numpy as np
+
+import gisspa
+import synth
+
+SCORE_RTOL = 1e-4   # plain FP32 form vs the FP64 oracle (relative)
+SCORE_ATOL = 2e-5   # absolute slack for scores near zero
+
+
+def config_from(cfg_dict: dict, **over) -> gisspa.Config:
+    d = dict(cfg_dict)
+    if "Highres" in d:
+        d["highres"] = d.pop("Highres")
+    if "Lowres" in d:
+        d["lowres"] = d.pop("Lowres")
+    d.update(over)
+    return gisspa.Config.default(**d)
+
+
+# Small cases (oracle runs in seconds); the reference's preconditions hold except where noted.
+SMALL = {
+    # whole-image norm_type=1, 3x3 windows, more windows than templates (padded templates count in N)
+    "norm_l256_w9": (dict(shape=(512, 512), n_particles=5, snr=0.6, n_templates=4, tsize=64, seed=21, defocus=1.5,
+                          dfdiff=0.08, dfang=35.0, margin=40),
+                     dict(angpix=1.0, phistep=45.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                          diameter=48.0, threshold=3.0, window_size=256, overlap=64, norm_type=1)),
+    # l = 512 windows on a 1024^2 micrograph
+    "norm_l512_w4": (dict(shape=(1024, 1024), n_particles=8, snr=0.5, n_templates=4, tsize=128, seed=22,
+                          defocus=1.8, dfdiff=0.1, dfang=30.0),
+                     dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                          diameter=100.0, threshold=3.0, window_size=512, overlap=0, norm_type=1)),
+    # norm_type=0 on 720^2 tiles of a 1024^2 micrograph with 512 windows (the tiled workload's geometry)
+    "nonorm_l512": (dict(shape=(1024, 1024), n_particles=10, snr=0.5, n_templates=4, tsize=128, seed=23,
+                         defocus=1.5, dfdiff=0.0, dfang=0.0),
+                    dict(angpix=1.0, phistep=45.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                         diameter=100.0, threshold=8.0, window_size=512, overlap=128, norm_type=0)),
+}
+
+
+def small_case(name: str):
+    data, cfg = SMALL[name]
+    c = synth.make_case(**data)
+    return c.image, c.templates, gisspa.Ctf(c.defocus, c.dfdiff, c.dfang), gisspa.Config.default(**cfg)
+
+
+def rel_err(a: np.ndarray, b: np.ndarray) -> float:
+    a = np.asarray(a, dtype=np.complex128 if np.iscomplexobj(a) or np.iscomplexobj(b) else np.float64)
+    b = np.asarray(b, dtype=a.dtype)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def half_spectrum(full: np.ndarray) -> np.ndarray:
+    """[n][ky][kx] full complex spectra -> [n][kx in 0..L/2][ky] (the library's kx-major layout)."""
+    L = full.shape[-1]
+    return np.ascontiguousarray(np.swapaxes(full[..., : L // 2 + 1], -1, -2))
+
+
+def compare_chunk_picks(gpu: np.ndarray, ref: np.ndarray, thresh: float, rtol=SCORE_RTOL, atol=SCORE_ATOL):
+    """Chunk picks must match by (angle, window, template, chunk) with scores within tolerance and
+    identical centres, except picks whose score lies within the tolerance of the threshold."""
+    key = lambda p: (int(p["angle_index"]), int(p["window"]), int(p["template_id"]), int(p["chunk"]))
+    G = {key(p): p for p in gpu}
+    R = {key(p): p for p in ref}
+    band = rtol * abs(thresh) + atol
+    report = dict(n_gpu=len(G), n_ref=len(R), missing=0, extra=0, score_bad=0, pos_bad=0, max_rel=0.0)
+    for k, r in R.items():
+        if k not in G:
+            if r["score"] >= thresh + band:
+                report["missing"] += 1
+            continue
+        g = G[k]
+        d = abs(float(g["score"]) - float(r["score"]))
+        report["max_rel"] = max(report["max_rel"], d / max(abs(float(r["score"])), 1e-9))
+        if d > rtol * abs(float(r["score"])) + atol:
+            report["score_bad"] += 1
+        if (g["x"], g["y"]) != (r["x"], r["y"]):
+            report["pos_bad"] += 1
+    for k, g in G.items():
+        if k not in R and g["score"] >= thresh + band:
+            report["extra"] += 1
+    return report
+
+
+def compare_template_picks(gpu: np.ndarray, ref: np.ndarray, thresh: float, rtol=SCORE_RTOL, atol=SCORE_ATOL,
+                           key_fields=("tile", "angle_index", "template_id")):
+    """norm_type=0 picks: one per (tile, angle, template); centre and score compared."""
+    key = lambda p: tuple(int(p[f]) for f in key_fields)
+    G = {key(p): p for p in gpu}
+    R = {key(p): p for p in ref}
+    band = rtol * abs(thresh) + atol
+    report = dict(n_gpu=len(G), n_ref=len(R), missing=0, extra=0, score_bad=0, pos_bad=0, max_rel=0.0)
+    for k, r in R.items():
+        if k not in G:
+            if r["score"] >= thresh + band:
+                report["missing"] += 1
+            continue
+        g = G[k]
+        d = abs(float(g["score"]) - float(r["score"]))
+        report["max_rel"] = max(report["max_rel"], d / max(abs(float(r["score"])), 1e-9))
+        if d > rtol * abs(float(r["score"])) + atol:
+            report["score_bad"] += 1
+        if abs(float(g["x"]) - float(r["x"])) > 1e-3 or abs(float(g["y"]) - float(r["y"])) > 1e-3:
+            report["pos_bad"] += 1
+    for k, g in G.items():
+        if k not in R and g["score"] >= thresh + band:
+            report["extra"] += 1
+    return report

@@ -1,0 +1,91 @@
+"""CPU checks of the C-ABI library: it loads, exports every declared symbol, parses the
+reference config format and formats pick lines; no device is needed."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import gisspa
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(REPO, "include", "gisspa.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gisspa_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = gisspa.load()
+    names = declared_functions()
+    assert len(names) >= 14
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(gisspa.SIGNATURES)
+
+
+def test_version():
+    assert b"sm_100a" in gisspa.load().gisspa_version()
+
+
+def test_config_defaults_match_reference():
+    c = gisspa.Config()
+    gisspa.load().gisspa_config_default(C.byref(c))
+    assert c.window_size == 320 and c.threshold == pytest.approx(7.0) and c.norm_type == 0
+    assert c.edge_half_width == 4.0 and c.ampconst == pytest.approx(0.07) and c.a == pytest.approx(-10.81)
+    assert c.quirks == gisspa.QUIRKS_REFERENCE and c.tile_size == 720
+
+
+def test_config_file_parsing(tmp_path):
+    p = tmp_path / "config"
+    p.write_text("input = mics.lst\ntemplate = t.hdf\neulerfile = e.txt\nangpix = 1.3\nphistep = 5\nkk = 3\n"
+                 "energy = 300\ncs = 2.7\nHighres = 8\nLowres = 200\ndiameter = 180\nthreshold = 7.5\n"
+                 "output = out.lst\nfirst = 2\nlast = 9\nGPU_ID = 1\nwindow_size = 512\nphase_flip = 1\n"
+                 "overlap = 192\nnorm_type = 1\ninvert = 1\nunknown_key = whatever\npick_mode = topk\n"
+                 "spectrum_precision = fp16\ntopk = 50\n")
+    c, r = gisspa.load_config(str(p))
+    assert (c.angpix, c.phistep, c.window_size, c.overlap, c.norm_type, c.invert) == (
+        pytest.approx(1.3), 5.0, 512, 192, 1, 1)
+    assert c.pick_mode == gisspa.PICK_TOPK and c.spectrum_precision == gisspa.SPEC_FP16 and c.topk == 50
+    assert r.input == b"mics.lst" and r.template_path == b"t.hdf" and (r.first, r.last, r.gpu_id) == (2, 9, 1)
+
+
+def test_config_errors(tmp_path):
+    with pytest.raises(gisspa.GisspaError) as e:
+        gisspa.load_config(str(tmp_path / "missing"))
+    assert e.value.status == gisspa.ERR_IO
+    p = tmp_path / "bad"
+    p.write_text("window_size = abc\n")
+    with pytest.raises(gisspa.GisspaError):
+        gisspa.load_config(str(p))
+
+
+def test_format_pick_matches_reference_line():
+    p = np.zeros(1, dtype=gisspa.PICK_DTYPE)[0]
+    p["score"], p["x"], p["y"], p["angle"] = 7.25, 100.0, 200.0, 355.0
+    line = gisspa.format_pick(p, 3, "mic.mrc", gisspa.Ctf(1.5, 0.1, 30.0), 12.0, 45.0)
+    assert line == ("3\tmic.mrc\tdefocus=1.500000\tdfdiff=0.100000\tdfang=30.000000\teuler=12.000000,45.000000,"
+                    "355.000000\tcenter=100.000000,200.000000\tscore=7.250000\n")
+
+
+def test_create_rejects_bad_configs():
+    lib = gisspa.load()
+    h = C.c_void_p()
+    for over in [dict(window_size=300), dict(window_size=320), dict(phistep=0.0), dict(overlap=600)]:
+        cfg = gisspa.Config.default(angpix=1.0, phistep=5.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0,
+                                    lowres=200.0, diameter=100.0, window_size=512, norm_type=1, **{})
+        for k, v in over.items():
+            setattr(cfg, k, v)
+        st = lib.gisspa_create(C.byref(cfg), 0, C.byref(h))
+        assert st in (gisspa.ERR_SHAPE, gisspa.ERR_UNSUPPORTED, gisspa.ERR_ARG), (over, st)
+        assert lib.gisspa_last_error(None)
+
+
+def test_null_handle_is_an_argument_error():
+    lib = gisspa.load()
+    n = C.c_size_t(0)
+    assert lib.gisspa_search(None, None, 0, 0, None, None, 0, C.byref(n)) == gisspa.ERR_ARG
+    assert lib.gisspa_set_templates(None, None, 0, 0, 0) == gisspa.ERR_ARG

@@ -1,0 +1,172 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the FP64 oracle, stage by stage
+and end to end, on small seeded cases."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import gisspa
+import oracle
+from parity import (SCORE_ATOL, SCORE_RTOL, compare_chunk_picks, compare_template_picks, half_spectrum, rel_err,
+                    small_case)
+
+pytestmark = pytest.mark.gpu
+
+
+def stage(s: gisspa.Searcher, what: int, image, ctf, theta: float, shape, dtype):
+    out = np.zeros(shape, dtype=dtype)
+    img_ptr, nx, ny = (None, 0, 0)
+    if image is not None:
+        image = np.ascontiguousarray(image, dtype=np.float32)
+        img_ptr, (ny, nx) = image.ctypes.data, image.shape
+    lib = gisspa.load()
+    st = lib.gisspa_debug_stage(s.h, what, img_ptr, nx, ny, C.byref(ctf), theta, out.ctypes.data, out.nbytes)
+    assert st == 0, lib.gisspa_last_error(s.h)
+    return out
+
+
+@pytest.fixture(scope="module")
+def norm_case():
+    img, tmpl, ctf, cfg = small_case("norm_l256_w9")
+    s = gisspa.Searcher(cfg)
+    s.set_templates(tmpl)
+    return img, tmpl, ctf, cfg, s
+
+
+def test_stage_templates_norm(norm_case):
+    img, tmpl, ctf, cfg, s = norm_case
+    L = cfg.window_size
+    g = stage(s, 1, None, ctf, 0.0, (tmpl.shape[0], L, L), np.float32)
+    o = oracle.prep_templates(cfg, ctf, tmpl).real
+    assert rel_err(g, o) < 1e-4
+
+
+def test_stage_image_norm(norm_case):
+    img, tmpl, ctf, cfg, s = norm_case
+    g = stage(s, 2, img, ctf, 0.0, img.shape, np.float32)
+    o = oracle.prep_image(cfg, ctf, img)
+    assert rel_err(g, o) < 1e-4
+
+
+def test_stage_window_spectra(norm_case):
+    img, tmpl, ctf, cfg, s = norm_case
+    L = cfg.window_size
+    o = oracle.window_spectra(cfg, oracle.prep_image(cfg, ctf, img))
+    g = stage(s, 3, img, ctf, 0.0, (o.shape[0], L // 2 + 1, L), np.complex64)
+    assert rel_err(g, half_spectrum(o)) < 1e-4
+
+
+@pytest.mark.parametrize("theta", [0.0, 45.0, 135.0])
+def test_stage_template_spectra(norm_case, theta):
+    img, tmpl, ctf, cfg, s = norm_case
+    L = cfg.window_size
+    prep = oracle.prep_templates(cfg, ctf, tmpl)
+    o = np.stack([oracle.rotated_spectrum(cfg, ctf, prep[n], theta) for n in range(tmpl.shape[0])])
+    g = stage(s, 4, None, ctf, theta, (tmpl.shape[0], L // 2 + 1, L), np.complex64)
+    assert rel_err(g, half_spectrum(o)) < 1e-4
+
+
+def test_cc_maps_against_oracle(norm_case):
+    """CC maps through gisspa_cc_maps: the hot correlation kernels on oracle spectra."""
+    torch = pytest.importorskip("torch")
+    img, tmpl, ctf, cfg, s = norm_case
+    L = cfg.window_size
+    win = oracle.window_spectra(cfg, oracle.prep_image(cfg, ctf, img))[:3]
+    prep = oracle.prep_templates(cfg, ctf, tmpl)
+    T = np.stack([oracle.rotated_spectrum(cfg, ctf, prep[n], 45.0) for n in range(2)])
+    dW = torch.from_numpy(half_spectrum(win).astype(np.complex64)).cuda()
+    dT = torch.from_numpy(half_spectrum(T).astype(np.complex64)).cuda()
+    out = torch.zeros((3, 2, L, L), dtype=torch.float32, device="cuda")
+    lib = gisspa.load()
+    st = lib.gisspa_cc_maps(s.h, dW.data_ptr(), 3, dT.data_ptr(), 2, gisspa.SPEC_FP32, out.data_ptr())
+    assert st == 0, lib.gisspa_last_error(s.h)
+    g = out.cpu().numpy()
+    yy, xx = np.mgrid[0:L, 0:L]
+    chk = np.where((xx + yy) % 2 == 1, -1.0, 1.0)
+    for b in range(3):
+        for n in range(2):
+            ref = np.fft.ifft2(win[b] * np.conj(T[n]) * chk).real  # = IFFT_unnormalised / L^2
+            assert rel_err(g[b, n], ref) < 1e-4, (b, n)
+
+
+def run_both(name, **over):
+    img, tmpl, ctf, cfg = small_case(name)
+    cfg = cfg.copy(**over)
+    s = gisspa.Searcher(cfg)
+    s.set_templates(tmpl)
+    g = s.search(img, ctf)
+    o = oracle.search(cfg, ctf, img, tmpl)
+    return g, o, cfg, s
+
+
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4"])
+def test_search_norm_chunk_picks(name):
+    g, o, cfg, s = run_both(name)
+    rep = compare_chunk_picks(g, o, cfg.threshold)
+    assert len(o) > 0
+    assert rep["missing"] == 0 and rep["extra"] == 0 and rep["score_bad"] == 0, rep
+    assert rep["pos_bad"] <= max(1, len(o) // 200), rep
+
+
+def test_search_norm_stats_maps():
+    img, tmpl, ctf, cfg = small_case("norm_l256_w9")
+    s = gisspa.Searcher(cfg)
+    s.set_templates(tmpl)
+    s.search(img, ctf)
+    picks, st = oracle.search(cfg, ctf, img, tmpl, want_stats=True)
+    W, L = st.shape[0], cfg.window_size
+    ms = stage(s, 5, None, ctf, 0.0, (W, L, L, 2), np.float32)
+    mu_o, sd_o = st[..., 0], st[..., 1]
+    assert np.abs(ms[..., 0] - mu_o).max() <= 1e-4 * np.abs(sd_o).max()
+    sd_g = np.where(ms[..., 1] > 0, 1.0 / np.maximum(ms[..., 1], 1e-30), 0.0)
+    assert rel_err(sd_g, sd_o) < 1e-4
+
+
+def test_search_norm_topk():
+    g, o, cfg, s = run_both("norm_l256_w9", pick_mode=gisspa.PICK_TOPK, topk=20, exclusion_radius=30.0,
+                            threshold=2.0)
+    assert len(o) > 0 and len(g) == len(o)
+    n_same = sum(1 for a, b in zip(g, o) if (a["x"], a["y"], a["template_id"], a["angle_index"]) ==
+                 (b["x"], b["y"], b["template_id"], b["angle_index"]))
+    assert n_same >= len(o) - 1, (g, o)
+    assert np.allclose(np.sort(g["score"]), np.sort(o["score"]), rtol=SCORE_RTOL, atol=SCORE_ATOL)
+
+
+def test_search_nonorm():
+    g, o, cfg, s = run_both("nonorm_l512")
+    rep = compare_template_picks(g, o, cfg.threshold)
+    assert len(o) > 0
+    assert rep["missing"] == 0 and rep["extra"] == 0 and rep["score_bad"] == 0, rep
+    assert rep["pos_bad"] <= max(1, len(o) // 100), rep
+
+
+@pytest.mark.parametrize("spec", [gisspa.SPEC_FP16, gisspa.SPEC_BF16])
+def test_half_precision_spectra_close(spec):
+    """FP16/BF16 template spectra: scores stay close to the FP64 oracle (looser bound)."""
+    g, o, cfg, s = run_both("norm_l256_w9", spectrum_precision=spec, pick_mode=gisspa.PICK_TOPK, topk=20,
+                            exclusion_radius=30.0, threshold=2.0)
+    tol = 2e-3 if spec == gisspa.SPEC_FP16 else 2e-2
+    assert np.allclose(np.sort(g["score"])[-5:], np.sort(o["score"])[-5:], rtol=tol)
+
+
+def test_search_host_and_device_paths_agree():
+    torch = pytest.importorskip("torch")
+    img, tmpl, ctf, cfg = small_case("norm_l256_w9")
+    s = gisspa.Searcher(cfg)
+    s.set_templates(tmpl)
+    a = s.search(img, ctf)
+    d = torch.from_numpy(img).cuda()
+    out = np.zeros(1 << 16, dtype=gisspa.PICK_DTYPE)
+    n = s.search_device(d.data_ptr(), img.shape[1], img.shape[0], ctf, out)
+    assert n == len(a) and np.array_equal(out[:n], a)
+
+
+def test_batch_matches_single_searches():
+    img, tmpl, ctf, cfg = small_case("norm_l256_w9")
+    img2 = np.ascontiguousarray(img[:, ::-1])
+    s = gisspa.Searcher(cfg)
+    s.set_templates(tmpl)
+    one = [s.search(img, ctf), s.search(img2, ctf)]
+    both = s.search_batch([img, img2], [ctf, ctf])
+    for x, y in zip(one, both):
+        assert np.array_equal(x, y)
