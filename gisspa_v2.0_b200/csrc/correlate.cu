@@ -203,7 +203,9 @@ __global__ void __launch_bounds__(NW * 32)
             z[i][h] = (c - ms[s][i][h].x) * ms[s][i][h].y;
             zmax = fmaxf(zmax, z[i][h]);
           }
-        if (team_any<TEAM>(zmax >= a.thresh)) {
+        // warp-uniform branch: the shuffles below use the full warp mask, so both
+        // half-warp teams (TEAM = 16) must enter together
+        if (__any_sync(0xffffffffu, zmax >= a.thresh)) {
           constexpr int CPR = L >= 256 ? L / 256 : 1;  // chunks per row
 #pragma unroll
           for (int ch = 0; ch < CPR; ++ch) {

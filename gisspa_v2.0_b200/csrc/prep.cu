@@ -399,8 +399,9 @@ __global__ void rotate_kernel(const float* __restrict__ in, int l, float cose, f
   if (id < l * l) {
     const int i = id % l, j = id / l;
     const float x = (float)(i - l / 2), y = (float)(j - l / 2);
-    const float x2 = __fadd_rn(__fadd_rn(__fmul_rn(cose, x), __fmul_rn(sine, y)), (float)(l / 2));
-    const float y2 = __fadd_rn(__fadd_rn(__fmul_rn(-sine, x), __fmul_rn(cose, y)), (float)(l / 2));
+    // same float expression as rotate_subIMG (kernels.cu:554-555)
+    const float x2 = (cose * x + sine * y) + l / 2;
+    const float y2 = (-sine * x + cose * y) + l / 2;
     if (!(x2 < 0 || x2 > l - 1.0f || y2 < 0 || y2 > l - 1.0f)) {
       const int ii = (int)floorf(x2), jj = (int)floorf(y2);
       int k0 = ii + jj * l, k1 = k0 + 1, k2 = k0 + l + 1, k3 = k0 + l;

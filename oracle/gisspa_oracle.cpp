@@ -422,13 +422,19 @@ void preprocess_image(const Params& p, std::vector<double>& img, int nx, int ny,
 
 // ------------------------------------------------------------------ rotation
 // rotate_subIMG (kernels.cu:534-603) of a real l x l image by theta degrees about (l/2, l/2).
+// The sampling coordinates are computed in float as the reference does (cos/sin in double,
+// rounded to float; x2 = (cose x + sine y) + l/2 in float): whether a border pixel is
+// interpolated or zeroed (x2 > l - 1) depends on that rounding at 90/180/270 degrees.
+// The interpolation itself is FP64.
 void rotate(const double* in, double* out, int l, float theta) {
-  double cose = std::cos((double)theta * REF_PI / 180), sine = std::sin((double)theta * REF_PI / 180);
+  const float cose = (float)std::cos((double)theta * REF_PI / 180), sine = (float)std::sin((double)theta * REF_PI / 180);
   for (int j = 0; j < l; ++j)
     for (int i = 0; i < l; ++i) {
-      double x = i - l / 2, y = j - l / 2;
-      double x2 = (cose * x + sine * y) + l / 2;
-      double y2 = (-sine * x + cose * y) + l / 2;
+      const float x = (float)(i - l / 2), y = (float)(j - l / 2);
+      volatile float a1 = cose * x, a2 = sine * y, b1 = -sine * x, b2 = cose * y;
+      volatile float s1 = a1 + a2, s2 = b1 + b2;
+      const float fx2 = s1 + (float)(l / 2), fy2 = s2 + (float)(l / 2);
+      double x2 = fx2, y2 = fy2;
       double res = 0;
       if (!(x2 < 0 || x2 > l - 1.0 || y2 < 0 || y2 > l - 1.0)) {
         int ii = (int)std::floor(x2), jj = (int)std::floor(y2);

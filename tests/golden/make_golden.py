@@ -26,47 +26,52 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-sys.path.insert(0, os.path.join(REPO, "gisspa_v2.0_b200"))
-import synth  # noqa: E402
+sys.path.insert(0, HERE)
+import fixture_data  # noqa: E402
 
 # Cases satisfy the reference's preconditions: window_size % 16 == 0, windows <= templates
 # (norm.cu:141-147 reads past the stack otherwise) and images >= 720 for norm_type=0.
 CASES = {
     "norm_512_l256": dict(
-        data=dict(shape=(512, 512), n_particles=5, snr=0.6, n_templates=4, tsize=64, seed=11, defocus=1.4,
-                  dfdiff=0.05, dfang=20.0, margin=40),
+        data=dict(shape=(512, 512), n_templates=4, tsize=64, n_blobs=12, n_particles=5, amp=0.6, seed=11, margin=40),
+        ctf=dict(defocus=1.4, dfdiff=0.05, dfang=20.0),
         outliers=[(30, 40, 25.0), (100, 300, -20.0), (400, 200, 12.0)],
         cfg=dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, Highres=8.0, Lowres=200.0, diameter=48.0,
                  threshold=3.7, window_size=256, overlap=0, norm_type=1, invert=0, phase_flip=0)),
     "norm_1024x768_l256": dict(
-        data=dict(shape=(768, 1024), n_particles=8, snr=0.6, n_templates=20, tsize=48, seed=12, defocus=2.1,
-                  dfdiff=0.15, dfang=70.0, margin=40),
+        data=dict(shape=(768, 1024), n_templates=20, tsize=48, n_blobs=10, n_particles=8, amp=0.6, seed=12,
+                  margin=40),
+        ctf=dict(defocus=2.1, dfdiff=0.15, dfang=70.0),
         outliers=[(5, 5, 30.0), (700, 500, -30.0)],
         cfg=dict(angpix=1.2, phistep=30.0, kk=2.0, energy=300.0, cs=2.7, Highres=9.0, Lowres=150.0, diameter=40.0,
                  threshold=4.3, window_size=256, overlap=32, norm_type=1, invert=0, phase_flip=0)),
     "nonorm_768_l256": dict(
-        data=dict(shape=(768, 768), n_particles=6, snr=0.6, n_templates=16, tsize=64, seed=13, defocus=1.6,
-                  dfdiff=0.0, dfang=0.0, margin=40),
+        data=dict(shape=(768, 768), n_templates=16, tsize=64, n_blobs=12, n_particles=6, amp=0.6, seed=13, margin=40),
+        ctf=dict(defocus=1.6, dfdiff=0.0, dfang=0.0),
         outliers=[],
         cfg=dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, Highres=8.0, Lowres=200.0, diameter=64.0,
-                 threshold=16.0, window_size=256, overlap=64, norm_type=0, invert=0, phase_flip=0)),
+                 threshold=7.3, window_size=256, overlap=64, norm_type=0, invert=0, phase_flip=0)),
     "nonorm_768_l256_flip": dict(
-        data=dict(shape=(768, 768), n_particles=6, snr=0.6, n_templates=16, tsize=64, seed=14, defocus=1.6,
-                  dfdiff=0.1, dfang=45.0, margin=40),
+        data=dict(shape=(768, 768), n_templates=16, tsize=64, n_blobs=12, n_particles=6, amp=0.6, seed=14, margin=40),
+        ctf=dict(defocus=1.6, dfdiff=0.1, dfang=45.0),
         outliers=[],
         cfg=dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, Highres=8.0, Lowres=200.0, diameter=64.0,
-                 threshold=8.0, window_size=256, overlap=64, norm_type=0, invert=1, phase_flip=1)),
+                 threshold=7.6, window_size=256, overlap=64, norm_type=0, invert=1, phase_flip=1)),
 }
 
 
+class _Ctf:
+    def __init__(self, defocus, dfdiff, dfang):
+        self.defocus, self.dfdiff, self.dfang = defocus, dfdiff, dfang
+
+
 def case_inputs(name: str):
-    """Deterministic inputs of a case: (image float32 [ny, nx], templates float32 [n, t, t], case dict)."""
+    """Bit-reproducible inputs of a case: (image float32 [ny, nx], templates float32 [n, t, t], CTF)."""
     spec = CASES[name]
-    c = synth.make_case(**spec["data"])
-    img = c.image.copy()
+    img, tmpl, _ = fixture_data.make_inputs(**spec["data"])
     for (x, y, v) in spec["outliers"]:
         img[y, x] = v
-    return img, c.templates, c
+    return img, tmpl, _Ctf(**spec["ctf"])
 
 
 def checksum(*arrays) -> str:

@@ -135,6 +135,7 @@ def test_search_norm_topk():
 def test_search_nonorm():
     g, o, cfg, s = run_both("nonorm_l512")
     rep = compare_template_picks(g, o, cfg.threshold)
+    print("nonorm report", rep)
     assert len(o) > 0
     assert rep["missing"] == 0 and rep["extra"] == 0 and rep["score_bad"] == 0, rep
     assert rep["pos_bad"] <= max(1, len(o) // 100), rep
