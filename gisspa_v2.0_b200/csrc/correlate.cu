@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
     pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
                   int b0, int n0, int D, const float2* __restrict__ twL) {
   constexpr int TT = PassA<L>::TT, NC = PassA<L>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
-  constexpr int PS = fft_padded_size(L);
+  constexpr int PS = L;
   __shared__ float2 smem[NC * PS];
   const int team = threadIdx.x / TT, tid = threadIdx.x - team * TT;
   const int c = blockIdx.x * NC + team;
@@ -86,11 +86,12 @@ __device__ __forceinline__ bool team_any(bool pred) {
 
 // Pass B: a team (TEAM lanes) per output row; RB rows per CTA, one window per blockIdx.y,
 // looping over the launch's D templates.
-template <int L, int TEAM, int RB, int NW, int EPI>
-__global__ void __launch_bounds__(NW * 32)
+template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB)
     pass_b_kernel(CorrArgs a, const float2* __restrict__ twL, const float2* __restrict__ twNZ) {
   constexpr int NZ = L / 2, E = NZ / TEAM, TPW = 32 / TEAM, NTEAM = NW * TPW, RPT = RB / NTEAM;
-  constexpr int RS = fft_padded_size(NZ);
+  // odd row stride: the staging stores (two rows per float4) hit distinct banks
+  constexpr int RS = NZ + 1;
   static_assert(RB % NTEAM == 0, "rows must split evenly over teams");
   static_assert(RB % 2 == 0, "float4 staging");
   __shared__ float2 stage[RB * RS];
@@ -342,28 +343,36 @@ void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, c
   GISSPA_LAUNCH_CHECK();
 }
 
-template <int L, int TEAM, int RB, int NW, int EPI>
+template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
 void launch_b_cfg(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ,
                   cudaStream_t s) {
   dim3 grid(L / RB, cl.E);
-  pass_b_kernel<L, TEAM, RB, NW, EPI><<<grid, NW * 32, 0, s>>>(args, twL, twNZ);
+  pass_b_kernel<L, TEAM, RB, NW, EPI, MINB><<<grid, NW * 32, 0, s>>>(args, twL, twNZ);
   GISSPA_LAUNCH_CHECK();
 }
 
-template <int L, int TEAM, int NW>
+// Pass B shapes (rows per CTA RB, warps NW, min CTAs per SM) per window size and variant.
+template <int L, int V>
+struct PassB;
+template <> struct PassB<256, 0> { static constexpr int TEAM = 16, RB = 16, NW = 8, MINB = 2; };
+template <> struct PassB<512, 0> { static constexpr int TEAM = 32, RB = 16, NW = 16, MINB = 1; };
+template <> struct PassB<512, 1> { static constexpr int TEAM = 32, RB = 8, NW = 8, MINB = 2; };
+template <> struct PassB<1024, 0> { static constexpr int TEAM = 32, RB = 8, NW = 8, MINB = 1; };
+
+template <int L, int V>
 void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ, cudaStream_t s) {
-  constexpr int NT = NW * (32 / TEAM);
+  using P = PassB<L, V>;
   switch (cl.epi) {
-    case EPI_SUM: launch_b_cfg<L, TEAM, (L == 512 ? 2 * NT : NT), NW, EPI_SUM>(cl, args, twL, twNZ, s); break;
-    case EPI_CHUNK: launch_b_cfg<L, TEAM, NT, NW, EPI_CHUNK>(cl, args, twL, twNZ, s); break;
-    case EPI_TOPK: launch_b_cfg<L, TEAM, NT, NW, EPI_TOPK>(cl, args, twL, twNZ, s); break;
-    case EPI_NONORM: launch_b_cfg<L, TEAM, NT, NW, EPI_NONORM>(cl, args, twL, twNZ, s); break;
-    case EPI_MAP: launch_b_cfg<L, TEAM, NT, NW, EPI_MAP>(cl, args, twL, twNZ, s); break;
+    case EPI_SUM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_SUM, P::MINB>(cl, args, twL, twNZ, s); break;
+    case EPI_CHUNK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_CHUNK, P::MINB>(cl, args, twL, twNZ, s); break;
+    case EPI_TOPK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_TOPK, P::MINB>(cl, args, twL, twNZ, s); break;
+    case EPI_NONORM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_NONORM, P::MINB>(cl, args, twL, twNZ, s); break;
+    case EPI_MAP: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_MAP, P::MINB>(cl, args, twL, twNZ, s); break;
     default: throw CudaError{cudaErrorInvalidValue, "unknown epilogue"};
   }
 }
 
-template <int L, int TEAM, int NW>
+template <int L>
 int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                 const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {
   if (ev) GISSPA_CUDA(cudaEventRecord(ev[0], s));
@@ -374,7 +383,14 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
     default: throw CudaError{cudaErrorInvalidValue, "unknown spectrum precision"};
   }
   if (ev) GISSPA_CUDA(cudaEventRecord(ev[1], s));
-  launch_b<L, TEAM, NW>(cl, args, twL, twNZ, s);
+  if constexpr (L == 512) {
+    if (cl.variant == 1)
+      launch_b<L, 1>(cl, args, twL, twNZ, s);
+    else
+      launch_b<L, 0>(cl, args, twL, twNZ, s);
+  } else {
+    launch_b<L, 0>(cl, args, twL, twNZ, s);
+  }
   if (ev) GISSPA_CUDA(cudaEventRecord(ev[2], s));
   return 2;
 }
@@ -383,12 +399,14 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
 
 bool correlate_supported(int L) { return L == 256 || L == 512 || L == 1024; }
 
+int correlate_variants(int L) { return L == 512 ? 2 : 1; }
+
 int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {
   switch (cl.L) {
-    case 256: return launch_pair<256, 16, 8>(cl, I, T, Q, args, twL, twNZ, s, ev);
-    case 512: return launch_pair<512, 32, 8>(cl, I, T, Q, args, twL, twNZ, s, ev);
-    case 1024: return launch_pair<1024, 32, 8>(cl, I, T, Q, args, twL, twNZ, s, ev);
+    case 256: return launch_pair<256>(cl, I, T, Q, args, twL, twNZ, s, ev);
+    case 512: return launch_pair<512>(cl, I, T, Q, args, twL, twNZ, s, ev);
+    case 1024: return launch_pair<1024>(cl, I, T, Q, args, twL, twNZ, s, ev);
     default: throw CudaError{cudaErrorInvalidValue, "window size without correlation kernels"};
   }
 }

@@ -70,6 +70,7 @@ struct CorrLaunch {
   int D;              // templates per window in this launch
   int spec;           // GISSPA_SPEC_*
   int epi;            // Epilogue
+  int variant = 0;    // pass B shape (see correlate_variants)
 };
 
 // Launch pass A then pass B on stream s.  I: window spectra [W][L/2+1][L];
@@ -81,5 +82,7 @@ int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float
 
 // Whether a window size has compiled correlation kernels.
 bool correlate_supported(int L);
+// Number of pass B shapes compiled for a window size (the autotuner's choices).
+int correlate_variants(int L);
 
 }  // namespace gisspa

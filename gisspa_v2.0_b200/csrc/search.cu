@@ -263,17 +263,87 @@ void template_spectra_at(Ctx& c, float theta) {
 
 void choose_batches(const gisspa_config& cfg, int l, int W, int nt, int& D, int& E) {
   const long long per_pair = (long long)(l / 2) * l * (long long)sizeof(float2);
-  const long long budget = 96LL << 20;
+  const long long budget = 64LL << 20;
   E = cfg.window_batch > 0 ? cfg.window_batch : (l >= 1024 ? 4 : 8);
   E = std::max(1, std::min(E, W));
   D = cfg.template_batch > 0 ? cfg.template_batch : (int)std::max(1LL, budget / per_pair / E);
   D = std::max(1, std::min(D, nt));
 }
 
+// Autotuner: times every candidate launch shape (pass B variant, template batch D, window
+// batch E) on the sweep's own spectra, with the epilogue's outputs redirected to scratch,
+// and keeps the fastest per (window size, epilogue, precision).
+TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int nt, CorrArgs args) {
+  gisspa_handle* h = c.h;
+  const int l = c.l;
+  struct Cand { int D, E; };
+  std::vector<Cand> cands;
+  if (l == 512) cands = {{8, 8}, {12, 8}, {6, 12}, {16, 6}, {4, 16}, {24, 4}, {10, 10}};
+  else if (l == 1024) cands = {{6, 4}, {4, 6}, {8, 3}, {12, 2}, {3, 8}, {4, 4}};
+  else cands = {{16, 8}, {32, 8}, {8, 16}, {64, 4}, {24, 12}};
+  int maxE = 1, maxDE = 1;
+  for (auto& cd : cands) {
+    cd.D = std::max(1, std::min(cd.D, nt));
+    cd.E = std::max(1, std::min(cd.E, W));
+    maxE = std::max(maxE, cd.E);
+    maxDE = std::max(maxDE, cd.D * cd.E);
+  }
+  // scratch outputs: S1, S2 (double), cmax (float), carg (int) for maxE windows; nn arrays; counter
+  const size_t px = (size_t)maxE * c.L2;
+  const size_t nn = (size_t)maxE * nt;
+  char* base = static_cast<char*>(h->tune_scratch.ensure(px * 24 + nn * 24 + 256));
+  args.S1 = reinterpret_cast<double*>(base);
+  args.S2 = args.S1 + px;
+  args.cmax = reinterpret_cast<float*>(args.S2 + px);
+  args.carg = reinterpret_cast<int*>(args.cmax + px);
+  args.nn_key = reinterpret_cast<unsigned long long*>(args.carg + px);
+  args.nn_sum = reinterpret_cast<double*>(args.nn_key + nn);
+  args.cand_count = reinterpret_cast<unsigned*>(args.nn_sum + 2 * nn);
+  args.cand_cap = 0;
+  args.cand = nullptr;
+  args.nt_total = nt;
+  float2* Q = buf<float2>(h->Q, (size_t)maxDE * (l / 2) * l);
+  args.Q = Q;
+  const float2* twL = h->fft.twiddles(l);
+  const float2* twNZ = h->fft.twiddles(l / 2);
+  TuneChoice best;
+  best.us_per_pair = 1e30;
+  for (int v = 0; v < correlate_variants(l); ++v)
+    for (const auto& cd : cands) {
+      CorrLaunch cl{l, cd.E, cd.D, h->cfg.spectrum_precision, epi, v};
+      args.b0 = 0;
+      args.n0 = 0;
+      args.D = cd.D;
+      correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s);
+      GISSPA_CUDA(cudaEventRecord(h->ev[5], c.s));
+      constexpr int kReps = 3;
+      for (int r = 0; r < kReps; ++r) correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s);
+      GISSPA_CUDA(cudaEventRecord(h->ev[6], c.s));
+      GISSPA_CUDA(cudaEventSynchronize(h->ev[6]));
+      float ms = 0;
+      GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
+      const double us = 1000.0 * ms / (kReps * cd.D * cd.E);
+      if (us < best.us_per_pair) best = TuneChoice{v, cd.D, cd.E, us};
+    }
+  return best;
+}
+
 // One correlation sweep at one angle over every (window, template) pair.
 long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, int nt, CorrArgs args, int D, int E) {
   gisspa_handle* h = c.h;
   const int l = c.l;
+  int variant = 0;
+  if (h->cfg.template_batch == 0 && h->cfg.window_batch == 0) {
+    const long long key = (long long)l | ((long long)epi << 16) | ((long long)h->cfg.spectrum_precision << 24) |
+                          ((long long)std::min(nt, 64) << 32) | ((long long)std::min(W, 64) << 40);
+    auto it = h->tuned.find(key);
+    if (it == h->tuned.end()) it = h->tuned.emplace(key, autotune(c, epi, I, W, T, nt, args)).first;
+    D = it->second.D;
+    E = it->second.E;
+    variant = it->second.variant;
+    h->st.pass_b_variant = variant;
+    h->st.tuned_us_per_pair = it->second.us_per_pair;
+  }
   float2* Q = buf<float2>(h->Q, (size_t)D * E * (l / 2) * l);
   const float2* twL = h->fft.twiddles(l);
   const float2* twNZ = h->fft.twiddles(l / 2);
@@ -282,8 +352,7 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
     const int d = std::min(D, nt - n0);
     for (int b0 = 0; b0 < W; b0 += E) {
       const int e = std::min(E, W - b0);
-      CorrLaunch cl{l, e, d, h->cfg.spectrum_precision, epi};
-      if (epi == EPI_NONORM) cl.spec = h->cfg.spectrum_precision;
+      CorrLaunch cl{l, e, d, h->cfg.spectrum_precision, epi, variant};
       args.Q = Q;
       args.b0 = b0;
       args.n0 = n0;

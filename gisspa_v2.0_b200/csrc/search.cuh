@@ -1,6 +1,7 @@
 // search.cuh — the search handle and the per-micrograph orchestration.
 #pragma once
 
+#include <map>
 #include <new>
 #include <string>
 #include <vector>
@@ -8,6 +9,14 @@
 #include "../../include/gisspa.h"
 #include "common.cuh"
 #include "fft_generic.cuh"
+
+namespace gisspa {
+// Correlation launch shape chosen by the autotuner for one (window size, epilogue, precision).
+struct TuneChoice {
+  int variant = 0, D = 1, E = 1;
+  double us_per_pair = 0;
+};
+}  // namespace gisspa
 
 struct gisspa_handle {
   gisspa_config cfg{};
@@ -38,6 +47,8 @@ struct gisspa_handle {
   gisspa::DevBuf Q, cand, cand_count, nn_key, nn_sum, zkey, zcand, zcount;
 
   gisspa_stats st{};
+  std::map<long long, gisspa::TuneChoice> tuned;
+  gisspa::DevBuf tune_scratch;
   // sampled per-launch timing of the correlation kernels
   static constexpr int kSamples = 64;
   cudaEvent_t sev[kSamples][3] = {};

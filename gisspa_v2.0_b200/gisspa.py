@@ -92,7 +92,8 @@ class Stats(C.Structure):
                 ("ms_sweep2", C.c_double), ("ms_pick", C.c_double), ("pairs", C.c_longlong),
                 ("kernel_launches", C.c_longlong), ("candidates", C.c_longlong), ("pass_a_us", C.c_double),
                 ("pass_b_us", C.c_double), ("pairs_per_launch", C.c_double), ("templates_per_launch", C.c_double),
-                ("pass_samples", C.c_int), ("window_size", C.c_int)]
+                ("pass_samples", C.c_int), ("window_size", C.c_int), ("pass_b_variant", C.c_int),
+                ("tuned_us_per_pair", C.c_double)]
 
 
 # Exported symbols and their ctypes signatures (kept in sync with include/gisspa.h).

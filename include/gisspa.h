@@ -116,6 +116,8 @@ typedef struct gisspa_stats {
   double templates_per_launch; /* mean template batch depth D of the sampled launches */
   int pass_samples;
   int window_size;
+  int pass_b_variant;          /* pass B shape picked by the autotuner (last sweep) */
+  double tuned_us_per_pair;    /* autotuner's measured time per pair of that shape */
 } gisspa_stats;
 
 typedef struct gisspa_handle gisspa_handle;
