@@ -20,19 +20,20 @@
 #include "prep.cuh"
 #include "search.cuh"
 
+namespace {
+thread_local std::string g_create_error;
+const char* kVersion = "gisspa-b200 0.1 (sm_100a)";
+}  // namespace
+
 namespace gisspa {
 long long& launch_counter() {
   static thread_local long long c = 0;
   return c;
 }
+void set_handleless_error(const std::string& msg) { g_create_error = msg; }
 }  // namespace gisspa
 
 using namespace gisspa;
-
-namespace {
-thread_local std::string g_create_error;
-const char* kVersion = "gisspa-b200 0.1 (sm_100a)";
-}  // namespace
 
 extern "C" {
 

@@ -115,6 +115,7 @@ SIGNATURES = {
     "gisspa_destroy": (None, [_P]),
     "gisspa_version": (C.c_char_p, []),
     "gisspa_cc_maps": (C.c_int, [_P, _P, C.c_int, _P, C.c_int, C.c_int, _P]),
+    "gisspa_cc_maps_noalloc": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "gisspa_debug_stage": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.POINTER(Ctf), C.c_float, _P,
                                      C.c_size_t]),
 }

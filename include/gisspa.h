@@ -184,6 +184,23 @@ const char* gisspa_version(void);
 int gisspa_cc_maps(gisspa_handle* h, const void* d_windows, int n_windows, const void* d_templates, int n_templates,
                    int spec, float* d_out);
 
+/* Correlation maps as gisspa_cc_maps, for callers that cannot allocate device memory
+ * (a framework that owns the device memory pool or budget, a locked-down allocator):
+ * this call makes no cudaMalloc/cudaFree or other allocating call.  No counterpart in
+ * the reference.  Its intermediate lives in a fixed 16 MiB __device__ array (plus a
+ * 15 KiB twiddle table) that every GPU loading the library holds until exit, so one
+ * call takes at most 16 MiB / (window_size^2 * 4 bytes) (window, template) pairs:
+ * 64 pairs at window_size 256, 16 at 512, 4 at 1024; larger calls return
+ * GISSPA_ERR_CAPACITY with the reason in gisspa_last_error(NULL).  d_windows,
+ * d_templates, d_out and window_size as for gisspa_cc_maps; runs on `stream`
+ * (a cudaStream_t, NULL = default stream) of the current device.  The first call on
+ * each device sets up that device's copy of the arrays (make that first call before
+ * any stream capture).  Every call shares the one intermediate, which is fully
+ * overwritten before it is read: calls that overlap on the GPU (other streams or
+ * threads) race on it and must be serialised by the caller. */
+int gisspa_cc_maps_noalloc(const void* d_windows, int n_windows, const void* d_templates, int n_templates,
+                           int window_size, int spec, float* d_out, void* stream);
+
 /* ---- diagnostics: stage outputs for parity tests (no counterpart in the reference) ---- */
 enum {
   GISSPA_STAGE_TEMPLATES = 1,        /* norm_type=1: float [nt][L][L] real-space prepared templates;
