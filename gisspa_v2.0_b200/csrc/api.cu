@@ -81,6 +81,9 @@ int gisspa_create(const gisspa_config* cfg, int device, gisspa_handle** out) {
     }
     GISSPA_CUDA(cudaSetDevice(device));
     GISSPA_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    GISSPA_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    GISSPA_CUDA(cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
+    GISSPA_CUDA(cudaEventCreateWithFlags(&h->ev_stats, cudaEventDisableTiming));
     for (auto& e : h->ev) GISSPA_CUDA(cudaEventCreate(&e));
     for (auto& r : h->sev)
       for (auto& e : r) GISSPA_CUDA(cudaEventCreate(&e));
@@ -196,6 +199,33 @@ int gisspa_search_batch(gisspa_handle* h, int n, const float* const* images, con
     if (st) return st;
   }
   return run_batch(h, n, images, nx, ny, ctfs, picks, cap, offsets);
+}
+
+int gisspa_score_grad(gisspa_handle* h, const gisspa_pick* picks, size_t n, const float* params,
+                      const gisspa_ctf* ctf, gisspa_grad* out) {
+  if (!h) return GISSPA_ERR_ARG;
+  if ((n && (!picks || !out))) {
+    h->err = "score_grad: null argument";
+    return GISSPA_ERR_ARG;
+  }
+  if (n == 0) return GISSPA_OK;
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    score_grad_run(h, picks, n, params, ctf, out);
+  });
+}
+
+int gisspa_refine(gisspa_handle* h, gisspa_pick* picks, size_t n, int steps, gisspa_ctf* ctf, float* params_out) {
+  if (!h) return GISSPA_ERR_ARG;
+  if ((n && !picks) || steps < 0) {
+    h->err = "refine: bad argument";
+    return GISSPA_ERR_ARG;
+  }
+  if (n == 0) return GISSPA_OK;
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    refine_run(h, picks, n, steps, ctf, params_out);
+  });
 }
 
 int gisspa_cc_maps(gisspa_handle* h, const void* d_windows, int n_windows, const void* d_templates, int n_templates,

@@ -20,15 +20,22 @@ template <> struct PassA<512> { static constexpr int TT = 64, NC = 8; };
 template <> struct PassA<1024> { static constexpr int TT = 64, NC = 4; };
 
 // Pass A: one team of TT threads per column slot, NC slots per CTA, one pair per blockIdx.y.
+// The column transforms leave row-major, Q[pair][y][slot], through a shared tile: each team
+// writes its column with the slot XOR-swizzled by the row (slot ^ (y mod NC)), and rows are
+// read back as 16-byte pairs, so both sides are free of bank conflicts and every row segment
+// of NC slots leaves as contiguous 16-byte stores.  The swizzle key is y >> SH with 16 / NC =
+// 2^SH rows per 128-byte line, so 16 consecutive rows of one column fall in 16 distinct bank
+// pairs.
 template <int L, typename SPEC>
 __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
     pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
                   int b0, int n0, int D, const float2* __restrict__ twL) {
   constexpr int TT = PassA<L>::TT, NC = PassA<L>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
-  constexpr int PS = L;
-  __shared__ float2 smem[NC * PS];
+  constexpr int SH = NC >= 16 ? 0 : NC == 8 ? 1 : 2;
+  static_assert(NC == 4 || NC == 8 || NC == 16, "swizzle assumes 4, 8 or 16 slots per CTA");
+  __shared__ __align__(16) float2 smem[NC * L];  // FFT exchange buffers, then the output tile
   const int team = threadIdx.x / TT, tid = threadIdx.x - team * TT;
-  const int c = blockIdx.x * NC + team;
+  const int c0 = blockIdx.x * NC, c = c0 + team;
   const int p = blockIdx.y;
   const int e = p / D, d = p - e * D;
   const float2* Ib = I + (size_t)(b0 + e) * HS * L;
@@ -39,8 +46,8 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
 #pragma unroll
     for (int i = 0; i < E; ++i) {
       const int ky = fft3_in_index<L, TT>(tid, i);
-      float2 a = cmulc(Ib[ky], SPEC::load(Tn + ky));
-      float2 b = cmulc(Ib[(size_t)NZ * L + ky], SPEC::load(Tn + (size_t)NZ * L + ky));
+      const float2 a = cmulc(Ib[ky], SPEC::load(Tn + ky));
+      const float2 b = cmulc(Ib[(size_t)NZ * L + ky], SPEC::load(Tn + (size_t)NZ * L + ky));
       v[i] = make_float2(a.x - b.y, a.y + b.x);
     }
   } else {
@@ -52,10 +59,22 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
       v[i] = cmulc(__ldg(Ic + ky), SPEC::load(Tc + ky));
     }
   }
-  fft3<L, TT, +1>(v, smem + team * PS, twL, tid, BlockSync{});
-  float2* Qp = Q + ((size_t)p * NZ + c) * L;
+  fft3<L, TT, +1>(v, smem + team * L, twL, tid, BlockSync{});
+  __syncthreads();
 #pragma unroll
-  for (int i = 0; i < E; ++i) Qp[fft3_out_index<L, TT>(tid, i)] = v[i];
+  for (int i = 0; i < E; ++i) {
+    const int y = fft3_out_index<L, TT>(tid, i);
+    smem[y * NC + (team ^ ((y >> SH) & (NC - 1)))] = v[i];
+  }
+  __syncthreads();
+  float2* Qp = Q + (size_t)p * L * NZ + c0;
+  constexpr int HALF = NC / 2;  // 16-byte pairs per row segment
+  for (int u = threadIdx.x; u < L * HALF; u += TT * NC) {
+    const int y = u / HALF, k = (u - y * HALF) * 2, sw = (y >> SH) & (NC - 1);
+    const float4 q = *reinterpret_cast<const float4*>(smem + y * NC + ((k ^ sw) & ~1));
+    *reinterpret_cast<float4*>(Qp + (size_t)y * NZ + k) =
+        (sw & 1) ? make_float4(q.z, q.w, q.x, q.y) : q;
+  }
 }
 
 template <int TEAM>
@@ -85,20 +104,36 @@ __device__ __forceinline__ bool team_any(bool pred) {
 }
 
 // Pass B: a team (TEAM lanes) per output row; RB rows per CTA, one window per blockIdx.y,
-// looping over the launch's D templates.
+// looping over the launch's D templates.  The RB rows of each template are one
+// contiguous block of Q: one bulk asynchronous copy per template into a
+// double-buffered shared stage, completed on an mbarrier, so the next template's rows
+// arrive while this one is transformed.  Every wait is bounded: on timeout the CTA
+// sets *a.err and leaves.
 template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB)
     pass_b_kernel(CorrArgs a, const float2* __restrict__ twL, const float2* __restrict__ twNZ) {
   constexpr int NZ = L / 2, E = NZ / TEAM, TPW = 32 / TEAM, NTEAM = NW * TPW, RPT = RB / NTEAM;
-  // odd row stride: the staging stores (two rows per float4) hit distinct banks
-  constexpr int RS = NZ + 1;
+  constexpr unsigned kStageBytes = RB * NZ * sizeof(float2);
   static_assert(RB % NTEAM == 0, "rows must split evenly over teams");
-  static_assert(RB % 2 == 0, "float4 staging");
-  __shared__ float2 stage[RB * RS];
+  extern __shared__ __align__(128) float2 stage[];  // [2][RB][NZ]
+  __shared__ __align__(8) uint64_t bars[2];
   const int team = threadIdx.x / TEAM, lt = threadIdx.x - team * TEAM;
   const int e = blockIdx.y, y0 = blockIdx.x * RB, win = a.b0 + e;
   const float inv = 1.0f / (float)(L * L);
   const size_t wbase = (size_t)win * L * L;
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int d) {
+    const float2* src = a.Q + ((size_t)(e * a.D + d) * L + y0) * NZ;
+    fence_proxy_async_smem();
+    mbar_expect_tx(&bars[d & 1], kStageBytes);
+    bulk_g2s(stage + (d & 1) * RB * NZ, src, kStageBytes, &bars[d & 1]);
+  };
+  if (threadIdx.x == 0) issue(0);
 
   // per-lane pixel coordinates: element i, half h -> (out_y of row s, out_x)
   int ox[E];
@@ -137,24 +172,30 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     }
   }
 
+  int issued = 1;
   for (int d = 0; d < a.D; ++d) {
     const int p = e * a.D + d;
-    const float2* Qp = a.Q + (size_t)p * NZ * L;
-    __syncthreads();
-    constexpr int UPC = RB / 2;
-    for (int u = threadIdx.x; u < NZ * UPC; u += NW * 32) {
-      const int c = u / UPC, yy = (u - c * UPC) * 2;
-      const float4 q = __ldg(reinterpret_cast<const float4*>(Qp + (size_t)c * L + y0 + yy));
-      stage[yy * RS + c] = make_float2(q.x, q.y);
-      stage[(yy + 1) * RS + c] = make_float2(q.z, q.w);
+    if (threadIdx.x == 0 && d + 1 < a.D) {
+      issue(d + 1);
+      ++issued;
     }
-    __syncthreads();
+    const bool ok = mbar_wait(&bars[d & 1], (d >> 1) & 1, 4000000000LL);
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) {
+        atomicOr(a.err, 1u);
+        // let copies already in flight land before the CTA's shared memory goes away
+        for (int k = d; k < issued; ++k) mbar_wait(&bars[k & 1], (k >> 1) & 1, 400000000LL);
+      }
+      __syncthreads();
+      return;
+    }
+    float2* stg = stage + (d & 1) * RB * NZ;
     double nn_s1 = 0.0, nn_s2 = 0.0;
 #pragma unroll
     for (int s = 0; s < RPT; ++s) {
       const int r = team + NTEAM * s;
       const int oy = (y0 + r + L / 2) & (L - 1);
-      float2* row = stage + r * RS;
+      float2* row = stg + r * NZ;
       float2 v[E];
 #pragma unroll
       for (int i = 0; i < E; ++i) {
@@ -302,6 +343,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         atomicAdd(a.nn_sum + 2 * q + 1, nn_s2);
       }
     }
+    __syncthreads();  // this stage buffer is refilled two templates later
   }
 
   if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
@@ -346,8 +388,15 @@ void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, c
 template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
 void launch_b_cfg(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ,
                   cudaStream_t s) {
+  constexpr size_t smem = 2 * (size_t)RB * (L / 2) * sizeof(float2);
+  static bool configured = false;
+  if (!configured) {
+    GISSPA_CUDA(cudaFuncSetAttribute(pass_b_kernel<L, TEAM, RB, NW, EPI, MINB>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
   dim3 grid(L / RB, cl.E);
-  pass_b_kernel<L, TEAM, RB, NW, EPI, MINB><<<grid, NW * 32, 0, s>>>(args, twL, twNZ);
+  pass_b_kernel<L, TEAM, RB, NW, EPI, MINB><<<grid, NW * 32, smem, s>>>(args, twL, twNZ);
   GISSPA_LAUNCH_CHECK();
 }
 

@@ -5,7 +5,7 @@
 // kx in [0, L/2] and ky in [0, L) ("kx-major"), the layout the column pass reads.
 //   pass A: for every pair and column kx: Z[ky] = I[kx][ky] conj(T[kx][ky]);
 //           columns 0 and L/2 (whose inverse transforms are real) are packed into
-//           one complex column; inverse FFT of length L along ky -> Q[pair][kx][y].
+//           one complex column; inverse FFT of length L along ky -> Q[pair][y][kx].
 //   pass B: per output row y, a length-L/2 complex inverse FFT turns the L/2+1
 //           Hermitian-half values into L real samples (even/odd interleave);
 //           the zero lag is moved to (L/2, L/2) (the reference's (-1)^(kx+ky)
@@ -35,7 +35,8 @@ struct Cand {
 };
 
 struct CorrArgs {
-  const float2* Q;          // pass A output, [pairs][L/2][L]
+  const float2* Q;          // pass A output, row-major [pairs][L][L/2] (slot 0 packs columns 0 and L/2)
+  unsigned* err;            // set to 1 when a bounded wait gives up
   int D;                    // templates per window in this launch
   int b0, n0;               // first window / template of the launch
   int angle;                // index of the angle in the angle sequence

@@ -24,6 +24,8 @@ static __device__ __align__(256) float2 g_noalloc_scratch[kNoAllocScratchBytes /
 // Twiddle tables exp(-2 pi i p / n) for n = 1024, 512, 256, 128, back to back.
 constexpr int kTwTotal = 1024 + 512 + 256 + 128;
 static __device__ __align__(256) float2 g_noalloc_twiddles[kTwTotal];
+// Set by a kernel whose bounded wait gave up; cleared by the call that reads it.
+static __device__ unsigned g_noalloc_flag;
 
 int tw_offset(int n) { return n == 1024 ? 0 : n == 512 ? 1024 : n == 256 ? 1536 : 1792; }
 
@@ -31,6 +33,7 @@ struct DeviceSlot {
   bool ready = false;
   float2* scratch = nullptr;
   float2* twiddles = nullptr;
+  unsigned* flag = nullptr;
 };
 std::mutex g_mu;
 DeviceSlot g_slots[64];
@@ -55,6 +58,12 @@ int setup(int dev, std::string& err) {
     return GISSPA_ERR_CUDA;
   }
   s.twiddles = static_cast<float2*>(p);
+  e = cudaGetSymbolAddress(&p, g_noalloc_flag);
+  if (e != cudaSuccess) {
+    err = std::string("cudaGetSymbolAddress(flag): ") + cudaGetErrorString(e);
+    return GISSPA_ERR_CUDA;
+  }
+  s.flag = static_cast<unsigned*>(p);
   float2 h[kTwTotal];
   for (int n : {1024, 512, 256, 128})
     for (int k = 0; k < n; ++k) {
@@ -115,6 +124,7 @@ static int cc_maps_noalloc(const void* d_windows, int n_windows, const void* d_t
   args.nt_real = n_templates;
   args.nt_total = n_templates;
   args.map_out = d_out;
+  args.err = ds.flag;
   CorrLaunch cl{L, n_windows, n_templates, spec, EPI_MAP, 0};
   try {
     correlate_launch(cl, static_cast<const float2*>(d_windows), d_templates, ds.scratch, args,

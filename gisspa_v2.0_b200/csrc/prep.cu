@@ -217,7 +217,7 @@ __global__ void apply_table_kernel(float2* __restrict__ F, int batch, int l, con
   F[i] = make_float2(v.x * w, v.y * w);
 }
 
-__global__ void rms_normalise_kernel(float2* __restrict__ F, int l) {
+__global__ void rms_normalise_kernel(float2* __restrict__ F, int l, double* __restrict__ factors) {
   __shared__ double sh[32];
   float2* G = F + (size_t)blockIdx.x * l * l;
   double s = 0, cnt = 0;
@@ -234,6 +234,7 @@ __global__ void rms_normalise_kernel(float2* __restrict__ F, int l) {
   s = block_sum(s, sh);
   cnt = block_sum(cnt, sh);
   const double m = sqrt(s / (cnt * cnt));
+  if (factors && threadIdx.x == 0) factors[blockIdx.x] = m;
   if (m == 0) return;
   const double inv = 1.0 / m;
   for (int i = threadIdx.x; i < l * l; i += blockDim.x) {
@@ -506,8 +507,8 @@ void apply_table(float2* F, int batch, int l, const float* table, cudaStream_t s
   GISSPA_LAUNCH_CHECK();
 }
 
-void rms_normalise(float2* F, int batch, int l, double*, cudaStream_t s) {
-  rms_normalise_kernel<<<batch, 512, 0, s>>>(F, l);
+void rms_normalise(float2* F, int batch, int l, double* factors, cudaStream_t s) {
+  rms_normalise_kernel<<<batch, 512, 0, s>>>(F, l, factors);
   GISSPA_LAUNCH_CHECK();
 }
 

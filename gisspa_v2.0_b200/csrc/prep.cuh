@@ -26,8 +26,9 @@ void mask_real(float2* data, int batch, int l, float d_m, float ehw, cudaStream_
 // band-pass x |CTF| x SSNR weight table for templates (apply_weighting_function kernels.cu:243-288)
 void tmpl_weight_table(float* table, int l, const DevParams& p, cudaStream_t s);
 void apply_table(float2* F, int batch, int l, const float* table, cudaStream_t s);
-// F /= sqrt(sum |F|^2 / count^2) over x <= l/2 and valid shells (kernels.cu:319-382 + host)
-void rms_normalise(float2* F, int batch, int l, double* scratch, cudaStream_t s);
+// F /= m, m = sqrt(sum |F|^2 / count^2) over x <= l/2 and valid shells (kernels.cu:319-382 +
+// host); m per batch entry is written to factors when not null
+void rms_normalise(float2* F, int batch, int l, double* factors, cudaStream_t s);
 void real_part(const float2* in, float* out, long long n, float scale, cudaStream_t s);
 void to_complex(const float* in, float2* out, long long n, cudaStream_t s);
 

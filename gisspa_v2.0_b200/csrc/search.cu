@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "correlate.cuh"
 #include "prep.cuh"
 #include "search.cuh"
@@ -199,10 +200,13 @@ void prepare_templates(Ctx& c) {
     mask_real(tb, nt, l, h->cfg.diameter, h->cfg.edge_half_width, c.s);
     h->fft.fft2(tb, tmp, nt, l, l, -1, 1.0f / (float)c.L2, c.s);
   }
+  if (h->keep_whitened && !nonorm)  // the adjoint differentiates the weighting applied next
+    GISSPA_CUDA(cudaMemcpyAsync(buf<float2>(h->tw_spec, (size_t)nt * c.L2), tb, sizeof(float2) * nt * c.L2,
+                                cudaMemcpyDeviceToDevice, c.s));
   float* table = buf<float>(h->table, c.L2);
   tmpl_weight_table(table, l, c.p, c.s);
   apply_table(tb, nt, l, table, c.s);
-  rms_normalise(tb, nt, l, nullptr, c.s);
+  rms_normalise(tb, nt, l, buf<double>(h->tmpl_m, nt), c.s);
   if (!nonorm) {
     h->fft.fft2(tb, tmp, nt, l, l, +1, 1.f, c.s);  // norm.cu:350-351, unnormalised
     real_part(tb, buf<float>(h->prep_real, (size_t)nt * c.L2), (long long)nt * c.L2, 1.f, c.s);
@@ -240,7 +244,7 @@ void window_spectra(Ctx& c, const float* img, int nx, int ny, const std::vector<
   float2* tmp = buf<float2>(h->win_tmp, (size_t)W * c.L2);
   gather_windows(img, nx, ny, dox, doy, bx, W, l, w, c.s);
   h->fft.fft2(w, tmp, W, l, l, -1, 1.0f / (float)c.L2, c.s);
-  rms_normalise(w, W, l, nullptr, c.s);
+  rms_normalise(w, W, l, buf<double>(h->win_m, W), c.s);
   h->fft.transpose(w, buf<float2>(h->ispec, (size_t)W * (l / 2 + 1) * l), W, l, l, c.s, l / 2 + 1);
 }
 
@@ -278,9 +282,10 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   const int l = c.l;
   struct Cand { int D, E; };
   std::vector<Cand> cands;
-  if (l == 512) cands = {{8, 8}, {12, 8}, {6, 12}, {16, 6}, {4, 16}, {24, 4}, {10, 10}};
-  else if (l == 1024) cands = {{6, 4}, {4, 6}, {8, 3}, {12, 2}, {3, 8}, {4, 4}};
-  else cands = {{16, 8}, {32, 8}, {8, 16}, {64, 4}, {24, 12}};
+  // (D, E): pass A runs L/2/NC x E CTAs, pass B L/RB x E; Q holds D x E pairs
+  if (l == 512) cands = {{8, 8}, {12, 8}, {6, 12}, {8, 12}, {4, 16}, {6, 16}, {16, 6}, {24, 4}};
+  else if (l == 1024) cands = {{6, 4}, {4, 6}, {3, 8}, {2, 12}, {4, 8}, {8, 3}, {2, 16}};
+  else cands = {{16, 8}, {32, 8}, {8, 16}, {16, 16}, {64, 4}};
   int maxE = 1, maxDE = 1;
   for (auto& cd : cands) {
     cd.D = std::max(1, std::min(cd.D, nt));
@@ -302,6 +307,7 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   args.cand_cap = 0;
   args.cand = nullptr;
   args.nt_total = nt;
+  args.err = h->dev_err.as<unsigned>();
   float2* Q = buf<float2>(h->Q, (size_t)maxDE * (l / 2) * l);
   args.Q = Q;
   const float2* twL = h->fft.twiddles(l);
@@ -347,6 +353,7 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
   float2* Q = buf<float2>(h->Q, (size_t)D * E * (l / 2) * l);
   const float2* twL = h->fft.twiddles(l);
   const float2* twNZ = h->fft.twiddles(l / 2);
+  args.err = h->dev_err.as<unsigned>();
   long long pairs = 0;
   for (int n0 = 0; n0 < nt; n0 += D) {
     const int d = std::min(D, nt - n0);
@@ -377,11 +384,17 @@ void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_
   const int l = c.l, nt = h->nt;
   const long long N = (long long)nx * ny;
   GISSPA_CUDA(cudaEventRecord(h->ev[0], c.s));
-  prepare_templates(c);
-  // micrograph
+  // LoadImage statistics on the side stream (the serial FP32 form occupies one SM for
+  // ~4 ns per pixel) while the templates are prepared on the main stream
   float* stats = buf<float>(h->stats, 4);
   double* scr = buf<double>(h->scratch, 16);
-  image_stats(d_img, nx, ny, (cfg.quirks & GISSPA_QUIRK_OUTLIER_FP32_SERIAL) != 0, stats, scr, c.s);
+  GISSPA_CUDA(cudaEventRecord(h->ev_in, c.s));
+  GISSPA_CUDA(cudaStreamWaitEvent(h->side, h->ev_in, 0));
+  image_stats(d_img, nx, ny, (cfg.quirks & GISSPA_QUIRK_OUTLIER_FP32_SERIAL) != 0, stats, scr, h->side);
+  GISSPA_CUDA(cudaEventRecord(h->ev_stats, h->side));
+  prepare_templates(c);
+  GISSPA_CUDA(cudaStreamWaitEvent(c.s, h->ev_stats, 0));
+  // micrograph
   float2* G = buf<float2>(h->img_c, N);
   image_load(d_img, N, stats, true, cfg.invert != 0, G, c.s);
   preprocess_full(c, G, nx, ny, true);
@@ -391,8 +404,15 @@ void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_
   const int bx = (int)ox.size(), W = bx * (int)oy.size();
   window_spectra(c, img, nx, ny, ox, oy);
   GISSPA_CUDA(cudaEventRecord(h->ev[1], c.s));
+  h->last_nx = nx;
+  h->last_ny = ny;
+  h->last_W = W;
+  h->last_bx = bx;
+  h->last_offx = ox;
+  h->last_offy = oy;
 
   const std::vector<float> angles = angle_list(cfg.phistep);
+  h->last_angles = angles;
   const int n_euler = (cfg.quirks & GISSPA_QUIRK_NEULER_TRUNC) ? (int)(360.0f / cfg.phistep) : (int)angles.size();
   const int batch = (cfg.quirks & GISSPA_QUIRK_COUNT_PADDED_TEMPLATES) ? std::max(nt, W) : nt;
   const double Ntot = (double)batch * n_euler;
@@ -762,6 +782,183 @@ void debug_stage(gisspa_handle* h, int what, const float* d_img, int nx, int ny,
   throw CudaError{cudaErrorInvalidValue, "debug_stage: unknown stage"};
 }
 
+// ---- adjoint (a-Adj): score gradients and refinement of picks and of the micrograph CTF
+namespace {
+
+struct Psi {
+  double dfu, dfv, dfang;
+};
+Psi psi_of(const gisspa_ctf& c) { return Psi{-c.defocus + c.dfdiff, -c.defocus - c.dfdiff, c.dfang}; }
+gisspa_ctf ctf_of(const Psi& p) { return gisspa_ctf{-(p.dfu + p.dfv) / 2, (p.dfu - p.dfv) / 2, p.dfang}; }
+
+// Prepared templates and their CTF derivatives at ctf; window sums of the last search.
+void adjoint_prepare(gisspa_handle* h, const gisspa_ctf& ctf) {
+  Ctx c{h, h->stream, h->cfg.window_size, (long long)h->cfg.window_size * h->cfg.window_size,
+        make_params(h->cfg, ctf)};
+  const int l = c.l, nt = h->nt;
+  h->keep_whitened = true;
+  prepare_templates(c);
+  h->keep_whitened = false;
+  float* dtab = buf<float>(h->dtab, 3 * (size_t)c.L2);
+  ctf_dweight(dtab, l, c.p, c.s);
+  float* dprep = buf<float>(h->dprep, 3 * (size_t)nt * c.L2);
+  float2* tb = buf<float2>(h->tb, (size_t)nt * c.L2);
+  float2* tmp = buf<float2>(h->tb_tmp, (size_t)nt * c.L2);
+  for (int q = 0; q < 3; ++q) {
+    scale_by_table(h->tw_spec.as<float2>(), dtab + (size_t)q * c.L2, h->tmpl_m.as<double>(), nt, l, tb, c.s);
+    h->fft.fft2(tb, tmp, nt, l, l, +1, 1.f, c.s);  // same unnormalised IFFT as the prepared templates
+    real_part(tb, dprep + (size_t)q * nt * c.L2, (long long)nt * c.L2, 1.f, c.s);
+  }
+  window_sums(h->img_pre.as<float>(), h->last_nx, h->last_ny, h->offx.as<int>(), h->offy.as<int>(), h->last_bx,
+              h->last_W, l, h->win_m.as<double>(), buf<double>(h->win_sum, h->last_W), c.s);
+}
+
+void eval_grads(gisspa_handle* h, const std::vector<GradPick>& gp, std::vector<float>& out) {
+  const int n = (int)gp.size();
+  GradArgs g{};
+  g.prep = h->prep_real.as<float>();
+  g.dprep = h->dprep.as<float>();
+  g.img = h->img_pre.as<float>();
+  g.nx = h->last_nx;
+  g.ny = h->last_ny;
+  g.offx = h->offx.as<int>();
+  g.offy = h->offy.as<int>();
+  g.bx = h->last_bx;
+  g.win_m = h->win_m.as<double>();
+  g.win_sum = h->win_sum.as<double>();
+  g.musig = h->musig.as<float2>();
+  g.L = h->cfg.window_size;
+  g.nt = h->nt;
+  g.d_m = h->cfg.diameter;
+  g.ehw = h->cfg.edge_half_width;
+  GradPick* dp = buf<GradPick>(h->grad_in, n);
+  float* dout = buf<float>(h->grad_out, (size_t)n * 7);
+  GISSPA_CUDA(cudaMemcpyAsync(dp, gp.data(), sizeof(GradPick) * n, cudaMemcpyHostToDevice, h->stream));
+  score_grads(g, dp, n, dout, h->stream);
+  out.resize((size_t)n * 7);
+  GISSPA_CUDA(cudaMemcpyAsync(out.data(), dout, sizeof(float) * n * 7, cudaMemcpyDeviceToHost, h->stream));
+  GISSPA_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+std::vector<GradPick> grad_picks(gisspa_handle* h, const gisspa_pick* picks, size_t n, const float* params) {
+  std::vector<GradPick> gp(n);
+  const int L = h->cfg.window_size;
+  for (size_t i = 0; i < n; ++i) {
+    const gisspa_pick& p = picks[i];
+    if (p.window < 0 || p.window >= h->last_W || p.template_id < 0 || p.template_id >= h->nt)
+      throw CudaError{cudaErrorInvalidValue, "pick " + std::to_string(i) + " does not belong to the last search"};
+    GradPick g{};
+    g.b = p.window;
+    g.n = p.template_id;
+    g.px = (int)p.x - h->last_offx[p.window % h->last_bx];
+    g.py = (int)p.y - h->last_offy[p.window / h->last_bx];
+    if (g.px < 0 || g.px >= L || g.py < 0 || g.py >= L)
+      throw CudaError{cudaErrorInvalidValue, "pick " + std::to_string(i) + " lies outside its window"};
+    g.dx = params ? params[3 * i] : 0.f;
+    g.dy = params ? params[3 * i + 1] : 0.f;
+    g.theta = params ? params[3 * i + 2] : p.theta;
+    gp[i] = g;
+  }
+  return gp;
+}
+
+}  // namespace
+
+void score_grad_run(gisspa_handle* h, const gisspa_pick* picks, size_t n, const float* params, const gisspa_ctf* ctf,
+                    gisspa_grad* out) {
+  if (h->last_W <= 0 || h->cfg.norm_type == 0)
+    throw CudaError{cudaErrorInvalidValue, "score gradients need a preceding norm_type=1 search on this handle"};
+  std::vector<GradPick> gp = grad_picks(h, picks, n, params);
+  adjoint_prepare(h, ctf ? *ctf : h->last_ctf);
+  std::vector<float> o;
+  eval_grads(h, gp, o);
+  for (size_t i = 0; i < n; ++i)
+    out[i] = gisspa_grad{o[7 * i], o[7 * i + 1], o[7 * i + 2], o[7 * i + 3], o[7 * i + 4], o[7 * i + 5], o[7 * i + 6]};
+}
+
+// Batched local refinement: per pick, normalised gradient ascent on (dx, dy, theta) with an
+// adaptive step (grown on success, halved on failure); per micrograph, the same on the CTF
+// (dfu, dfv, dfang) driven by the summed pick gradients.  Each proposal is evaluated and kept
+// only if it raises the score (mean score for the CTF).
+void refine_run(gisspa_handle* h, gisspa_pick* picks, size_t n, int steps, gisspa_ctf* ctf, float* params_out) {
+  if (h->last_W <= 0 || h->cfg.norm_type == 0)
+    throw CudaError{cudaErrorInvalidValue, "refinement needs a preceding norm_type=1 search on this handle"};
+  std::vector<GradPick> gp = grad_picks(h, picks, n, nullptr);
+  Psi psi = psi_of(ctf ? *ctf : h->last_ctf);
+  adjoint_prepare(h, ctf_of(psi));
+  std::vector<float> cur, trial;
+  eval_grads(h, gp, cur);
+  std::vector<double> eps(n, 1.0);
+  double eps_psi = 1.0;
+  const double eta[3] = {1.0, 1.0, std::max(0.5, 0.5 * (double)h->cfg.phistep)};
+  const double eta_psi[3] = {0.05, 0.05, 5.0};
+  auto mean_score = [&](const std::vector<float>& v) {
+    double s = 0;
+    for (size_t i = 0; i < n; ++i) s += v[7 * i];
+    return n ? s / n : 0.0;
+  };
+  for (int it = 0; it < steps; ++it) {
+    // picks
+    std::vector<GradPick> prop = gp;
+    for (size_t i = 0; i < n; ++i) {
+      const double g[3] = {cur[7 * i + 1] * eta[0], cur[7 * i + 2] * eta[1], cur[7 * i + 3] * eta[2]};
+      const double nrm = std::sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+      if (!(nrm > 0)) continue;
+      prop[i].dx = (float)(gp[i].dx + eps[i] * eta[0] * g[0] / nrm);
+      prop[i].dy = (float)(gp[i].dy + eps[i] * eta[1] * g[1] / nrm);
+      prop[i].theta = (float)(gp[i].theta + eps[i] * eta[2] * g[2] / nrm);
+    }
+    eval_grads(h, prop, trial);
+    for (size_t i = 0; i < n; ++i) {
+      if (trial[7 * i] > cur[7 * i]) {
+        gp[i] = prop[i];
+        for (int k = 0; k < 7; ++k) cur[7 * i + k] = trial[7 * i + k];
+        eps[i] = std::min(eps[i] * 1.25, 4.0);
+      } else {
+        eps[i] *= 0.5;
+      }
+    }
+    // micrograph CTF (only when the caller passes one to refine)
+    if (!ctf) continue;
+    double G[3] = {0, 0, 0};
+    for (size_t i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) G[k] += cur[7 * i + 4 + k] * eta_psi[k];
+    const double nrm = std::sqrt(G[0] * G[0] + G[1] * G[1] + G[2] * G[2]);
+    if (nrm > 0 && n) {
+      Psi p2{psi.dfu + eps_psi * eta_psi[0] * G[0] / nrm, psi.dfv + eps_psi * eta_psi[1] * G[1] / nrm,
+             psi.dfang + eps_psi * eta_psi[2] * G[2] / nrm};
+      adjoint_prepare(h, ctf_of(p2));
+      eval_grads(h, gp, trial);
+      if (mean_score(trial) > mean_score(cur)) {
+        psi = p2;
+        cur = trial;
+        eps_psi = std::min(eps_psi * 1.25, 4.0);
+      } else {
+        eps_psi *= 0.5;
+        adjoint_prepare(h, ctf_of(psi));
+      }
+    }
+  }
+  const int L = h->cfg.window_size;
+  (void)L;
+  for (size_t i = 0; i < n; ++i) {
+    picks[i].x += gp[i].dx;
+    picks[i].y += gp[i].dy;
+    picks[i].theta = gp[i].theta;
+    float cur_e = 360.0f - gp[i].theta;
+    while (cur_e >= 360.0f) cur_e -= 360.0f;
+    while (cur_e < 0.0f) cur_e += 360.0f;
+    picks[i].angle = cur_e;
+    picks[i].score = cur[7 * i];
+    if (params_out) {
+      params_out[3 * i] = gp[i].dx;
+      params_out[3 * i + 1] = gp[i].dy;
+      params_out[3 * i + 2] = gp[i].theta;
+    }
+  }
+  if (ctf) *ctf = ctf_of(psi);
+}
+
 void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int ntm, int spec, float* d_out) {
   Ctx c{h, h->stream, h->cfg.window_size, (long long)h->cfg.window_size * h->cfg.window_size, DevParams{}};
   const int l = c.l;
@@ -769,6 +966,8 @@ void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int n
   args.map_out = d_out;
   args.nt_real = ntm;
   args.nt_total = ntm;
+  args.err = buf<unsigned>(h->dev_err, 1);
+  GISSPA_CUDA(cudaMemsetAsync(args.err, 0, sizeof(unsigned), c.s));
   float2* Q = buf<float2>(h->Q, (size_t)ntm * (l / 2) * l);
   const float2* twL = h->fft.twiddles(l);
   const float2* twNZ = h->fft.twiddles(l / 2);
@@ -783,22 +982,32 @@ void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int n
     correlate_launch(cl, static_cast<const float2*>(d_win), d_t, Q, args, twL, twNZ, c.s);
   }
   GISSPA_CUDA(cudaStreamSynchronize(c.s));
+  unsigned flag = 0;
+  GISSPA_CUDA(cudaMemcpy(&flag, args.err, sizeof(flag), cudaMemcpyDeviceToHost));
+  if (flag) throw TimeoutError{"cc_maps"};
 }
 
 void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const gisspa_ctf& ctf,
                 std::vector<gisspa_pick>& out) {
   Ctx c{h, h->stream, h->cfg.window_size, (long long)h->cfg.window_size * h->cfg.window_size,
         make_params(h->cfg, ctf)};
+  h->last_ctf = ctf;
+  h->last_W = 0;
   const long long l0 = launch_counter();
   h->st = gisspa_stats{};
   h->n_samples = 0;
   h->launch_index = 0;
+  unsigned* err = buf<unsigned>(h->dev_err, 1);
+  GISSPA_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), c.s));
   if (h->cfg.norm_type != 0)
     search_norm(c, d_img, nx, ny, out);
   else
     search_nonorm(c, d_img, nx, ny, out);
   GISSPA_CUDA(cudaEventRecord(h->ev[4], c.s));
   GISSPA_CUDA(cudaStreamSynchronize(c.s));
+  unsigned flag = 0;
+  GISSPA_CUDA(cudaMemcpy(&flag, err, sizeof(flag), cudaMemcpyDeviceToHost));
+  if (flag) throw TimeoutError{"the correlation kernels"};
   float ms = 0;
   GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[0], h->ev[4]));
   h->st.ms_total = ms;

@@ -22,7 +22,9 @@ struct gisspa_handle {
   gisspa_config cfg{};
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // the serial LoadImage statistics overlap template preparation here
   cudaEvent_t ev[8] = {};
+  cudaEvent_t ev_in = nullptr, ev_stats = nullptr;
   std::string err;
   gisspa::FftEngine fft;
 
@@ -45,6 +47,15 @@ struct gisspa_handle {
   gisspa::DevBuf S1, S2, cmax, carg, musig;
   // correlation intermediate and outputs
   gisspa::DevBuf Q, cand, cand_count, nn_key, nn_sum, zkey, zcand, zcount;
+  gisspa::DevBuf dev_err;  // set by kernels whose bounded waits gave up
+  // adjoint: whitened template spectra before weighting, RMS factors, dW/dpsi tables,
+  // d(prepared template)/dpsi, window RMS factors and sums
+  gisspa::DevBuf tw_spec, tmpl_m, dtab, dprep, win_m, win_sum, grad_in, grad_out;
+  bool keep_whitened = false;
+  int last_nx = 0, last_ny = 0, last_W = 0, last_bx = 0;
+  gisspa_ctf last_ctf{};
+  std::vector<int> last_offx, last_offy;
+  std::vector<float> last_angles;
 
   gisspa_stats st{};
   std::map<long long, gisspa::TuneChoice> tuned;
@@ -62,6 +73,9 @@ struct gisspa_handle {
     for (auto& r : sev)
       for (auto& e : r)
         if (e) cudaEventDestroy(e);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_stats) cudaEventDestroy(ev_stats);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -72,12 +86,19 @@ namespace gisspa {
 int validate_config(const gisspa_config& c, std::string& err);
 int validate_image(const gisspa_config& c, int nx, int ny, std::string& err);
 
+struct TimeoutError {
+  std::string where;
+};
+
 // Runs fn, turning CUDA and allocation failures into status codes + h->err.
 template <typename F>
 int guarded(gisspa_handle* h, F&& fn) {
   try {
     fn();
     return GISSPA_OK;
+  } catch (const TimeoutError& e) {
+    h->err = "a bounded device wait gave up in " + e.where;
+    return GISSPA_ERR_TIMEOUT;
   } catch (const CudaError& e) {
     h->err = std::string(cudaGetErrorString(e.code)) + " at " + e.where;
     cudaGetLastError();
@@ -96,6 +117,9 @@ int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx
 void debug_stage(gisspa_handle* h, int what, const float* d_img, int nx, int ny, const gisspa_ctf& ctf, float theta,
                  void* out, size_t bytes);
 void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int ntm, int spec, float* d_out);
+void score_grad_run(gisspa_handle* h, const gisspa_pick* picks, size_t n, const float* params, const gisspa_ctf* ctf,
+                    gisspa_grad* out);
+void refine_run(gisspa_handle* h, gisspa_pick* picks, size_t n, int steps, gisspa_ctf* ctf, float* params_out);
 
 // Window offsets along one axis (blocks_one_axis, norm.cu:68-81).
 std::vector<int> window_offsets(int len, int l, int ov);

@@ -82,6 +82,13 @@ PICK_DTYPE = np.dtype([("score", "<f4"), ("x", "<f4"), ("y", "<f4"), ("angle", "
 assert PICK_DTYPE.itemsize == C.sizeof(Pick)
 
 
+class Grad(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("score", "d_dx", "d_dy", "d_theta", "d_dfu", "d_dfv", "d_dfang")]
+
+
+GRAD_DTYPE = np.dtype([(n, "<f4") for n in ("score", "d_dx", "d_dy", "d_theta", "d_dfu", "d_dfv", "d_dfang")])
+
+
 class RunPaths(C.Structure):
     _fields_ = [("input", C.c_char * 1024), ("template_path", C.c_char * 1024), ("eulerfile", C.c_char * 1024),
                 ("output", C.c_char * 1024), ("first", C.c_int), ("last", C.c_int), ("gpu_id", C.c_int)]
@@ -114,6 +121,8 @@ SIGNATURES = {
     "gisspa_last_error": (C.c_char_p, [_P]),
     "gisspa_destroy": (None, [_P]),
     "gisspa_version": (C.c_char_p, []),
+    "gisspa_score_grad": (C.c_int, [_P, _P, C.c_size_t, _P, C.POINTER(Ctf), _P]),
+    "gisspa_refine": (C.c_int, [_P, _P, C.c_size_t, C.c_int, C.POINTER(Ctf), _P]),
     "gisspa_cc_maps": (C.c_int, [_P, _P, C.c_int, _P, C.c_int, C.c_int, _P]),
     "gisspa_cc_maps_noalloc": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "gisspa_debug_stage": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.POINTER(Ctf), C.c_float, _P,
@@ -216,6 +225,27 @@ class Searcher:
         _check(self.h, st)
         o = list(offs)
         return [out[o[i]:o[i + 1]].copy() for i in range(n)]
+
+    def score_grad(self, picks: np.ndarray, params: np.ndarray | None = None, ctf: Ctf | None = None) -> np.ndarray:
+        """Scores and gradients of picks from the last norm_type=1 search (gisspa_score_grad)."""
+        picks = np.ascontiguousarray(picks, dtype=PICK_DTYPE)
+        out = np.zeros(len(picks), dtype=GRAD_DTYPE)
+        pp = None
+        if params is not None:
+            params = np.ascontiguousarray(params, dtype=np.float32).reshape(len(picks), 3)
+            pp = params.ctypes.data
+        _check(self.h, self.lib.gisspa_score_grad(self.h, picks.ctypes.data, len(picks), pp,
+                                                  C.byref(ctf) if ctf is not None else None, out.ctypes.data))
+        return out
+
+    def refine(self, picks: np.ndarray, steps: int = 20, ctf: Ctf | None = None):
+        """Refined copies of picks and the refined CTF (gisspa_refine)."""
+        picks = np.ascontiguousarray(picks, dtype=PICK_DTYPE).copy()
+        c = Ctf(ctf.defocus, ctf.dfdiff, ctf.dfang) if ctf is not None else None
+        params = np.zeros((len(picks), 3), np.float32)
+        _check(self.h, self.lib.gisspa_refine(self.h, picks.ctypes.data, len(picks), steps,
+                                              C.byref(c) if c is not None else None, params.ctypes.data))
+        return picks, c, params
 
     def stats(self) -> Stats:
         s = Stats()

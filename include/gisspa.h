@@ -174,6 +174,31 @@ void gisspa_destroy(gisspa_handle* h);
 /* Library version string. */
 const char* gisspa_version(void);
 
+/* Gradient of a pick's normalised score z = (c - mu)/sigma (no counterpart in the
+ * reference).  mu and sigma are held at the pick pixel; the shift moves the template's
+ * sampling (a Fourier shift on the periodic window), theta acts through the bilinear
+ * rotation, and the CTF through the template-side |CTF| x SSNR weight (the micrograph's
+ * preprocessing keeps the search's CTF). */
+typedef struct gisspa_grad {
+  float score;          /* z at the evaluated parameters */
+  float d_dx, d_dy;     /* per pixel of shift of the pick centre */
+  float d_theta;        /* per degree of the search angle theta (the printed angle is 360 - theta) */
+  float d_dfu, d_dfv;   /* per micrometre of the SetParams defocus_u / defocus_v (norm.cu:188-189) */
+  float d_dfang;        /* per degree of the astigmatism angle */
+} gisspa_grad;
+
+/* Scores and gradients of picks returned by the last norm_type=1 search on this handle.
+ * params: n x (dx, dy, theta) floats, or NULL for (0, 0, pick.theta); ctf: the CTF to
+ * evaluate the template weight at, or NULL for the search's. */
+int gisspa_score_grad(gisspa_handle* h, const gisspa_pick* picks, size_t n, const float* params,
+                      const gisspa_ctf* ctf, gisspa_grad* out);
+
+/* Batched local refinement of those picks (centre, theta) and of the micrograph CTF by
+ * gradient ascent for `steps` steps; picks (x, y, theta, angle, score) and *ctf are updated
+ * in place (ctf NULL: keep the search's CTF fixed and refine the picks only).  params_out
+ * (optional): n x (dx, dy, theta) relative to the input picks' centres. */
+int gisspa_refine(gisspa_handle* h, gisspa_pick* picks, size_t n, int steps, gisspa_ctf* ctf, float* params_out);
+
 /* Correlation maps of every (window, template) pair of device-resident half spectra
  * (compute_corner_CCG kernels.cu:645-678 + cufftExecC2C norm.cu:532-537, real part / L^2).
  * d_windows: n_windows x (L/2+1) x L complex FP32, kx-major (S[kx][ky]);

@@ -132,3 +132,69 @@ def tiles(width: int, height: int, tile: int = 720):
 
 def num_threads() -> int:
     return load().orc_num_threads()
+
+
+# ---------------------------------------------------------------- adjoint checker (FP64)
+REF_PI = 3.1415926535  # utils/constants.h:3
+
+
+def _shell_index(a, b):
+    n = a.astype(np.int64) ** 2 + b.astype(np.int64) ** 2
+    k = np.floor(np.sqrt(n.astype(np.float64)) + 0.5).astype(np.int64)
+    k = np.where((k > 0) & (k * k - k >= n), k - 1, k)
+    k = np.where(k * k + k < n, k + 1, k)
+    return k - 1
+
+
+def window_rms_factor(win: np.ndarray) -> float:
+    """Radial RMS factor m of one real window (norm.cu:431-466): F = FFT/L^2,
+    m = sqrt(sum |F|^2 / count^2) over x <= L/2 and valid shells."""
+    L = win.shape[0]
+    F = np.fft.fft2(win) / (L * L)
+    y, x = np.mgrid[0:L, 0:L]
+    r = _shell_index(np.minimum(y, L - y), np.minimum(x, L - x))
+    sel = (x <= L // 2) & (r >= 0) & (r < L // 2)
+    return float(np.sqrt(np.sum(np.abs(F[sel]) ** 2) / sel.sum() ** 2))
+
+
+def pick_score(cfg, prep_t: np.ndarray, img_pre: np.ndarray, off: tuple, px: int, py: int, dx: float, dy: float,
+               theta: float, mu: float, sigma: float) -> float:
+    """FP64 restatement of the score the adjoint differentiates (z of one pick at a continuous
+    shift (dx, dy) and search angle theta), from a prepared real-space template prep_t
+    [L, L] (the CTF enters through it) and the preprocessed micrograph.
+
+    c = (1/L^2) sum_y W(y + p + L/2) n(y - d), W = window / (L^2 m), n = the rotated (bilinear,
+    reference boundary rules), masked, mean/variance-normalised template; z = (c - mu)/sigma."""
+    L = cfg.window_size
+    ox, oy = off
+    ny, nx = img_pre.shape
+    win = np.zeros((L, L))
+    h_, w_ = min(L, ny - oy), min(L, nx - ox)
+    win[:h_, :w_] = img_pre[oy:oy + h_, ox:ox + w_]
+    W = win / (L * L * window_rms_factor(win))
+    Y, X = np.mgrid[0:L, 0:L].astype(np.float64)
+    ux, uy = X - (L // 2 + dx), Y - (L // 2 + dy)
+    r = np.hypot(ux, uy)
+    dm = 1.5 * cfg.diameter
+    r_in, r_out = dm / 2, dm / 2 + 2 * cfg.edge_half_width
+    m = np.where(r > r_out, 0.0, np.where(r >= r_in, 0.5 * np.cos(REF_PI * (r - r_in) / (2 * cfg.edge_half_width)) + 0.5,
+                                          1.0))
+    th = theta * REF_PI / 180
+    cs, sn = np.cos(th), np.sin(th)
+    x2 = cs * ux + sn * uy + L // 2
+    y2 = -sn * ux + cs * uy + L // 2
+    inside = ~((x2 < 0) | (x2 > L - 1.0) | (y2 < 0) | (y2 > L - 1.0))
+    x2c, y2c = np.where(inside, x2, 0.0), np.where(inside, y2, 0.0)
+    ii, jj = np.floor(x2c).astype(int), np.floor(y2c).astype(int)
+    i1 = np.where(ii == L - 1, ii, ii + 1)
+    j1 = np.where(jj == L - 1, jj, jj + 1)
+    t, u = x2c - ii, y2c - jj
+    P = prep_t
+    R = (P[jj, ii] * (1 - t) * (1 - u) + P[jj, i1] * t * (1 - u) + P[j1, i1] * t * u + P[j1, ii] * (1 - t) * u)
+    a = np.where(inside, m * R, 0.0)
+    mean = a.sum() / (L * L)
+    sd = np.sqrt((a * a).sum() / (L * L) - mean * mean)
+    n = (a - mean) / sd
+    Ws = np.roll(W, shift=(-(py + L // 2), -(px + L // 2)), axis=(0, 1))  # W(y + p + L/2)
+    c = float((Ws * n).sum()) / (L * L)
+    return (c - mu) / sigma

@@ -1,0 +1,141 @@
+"""Adjoint of the normalised score (gisspa_score_grad / gisspa_refine): consistency with the
+search, central finite differences through a torch.autograd.Function harness, and the
+refinement."""
+import numpy as np
+import pytest
+
+import gisspa
+import oracle
+from parity import small_case
+
+pytestmark = pytest.mark.gpu
+
+FD_H = 1e-3       # pick parameters: pixel, degree
+GRAD_RTOL = 1e-3  # adjoint vs FP64 central differences, relative to the gradient norm
+# Central differences of the library's own FP32 scores are limited twice over: rounding noise of
+# about 1e-6 relative in each score (2e-3 of a typical gradient at FD_H = 1e-3), and the kinks of
+# bilinear sampling, which make the score piecewise smooth, so a wider stencil averages slopes
+# across cell edges (a 9-point fit over +-4e-3 is 4e-3 off on dy).  This harness therefore holds
+# 1e-2; the 1e-3 bar is held against the FP64 oracle below.
+FD32_RTOL = 1e-2
+# The CTF components are checked against the FP64 oracle's central differences at h = 1e-5
+# (micrometre, degree): the template weight holds |CTF|, which has a kink at every CTF zero
+# ring, so a 1e-3 um central difference is dominated by its truncation error (measured 45 %
+# off on dfu), while FP32 evaluations on the GPU cannot resolve h = 1e-5.
+
+
+INPUTS = {}
+
+
+@pytest.fixture(scope="module")
+def searched():
+    img, tmpl, ctf, cfg = small_case("norm_l256_w9")
+    cfg = cfg.copy(pick_mode=gisspa.PICK_TOPK, topk=12, exclusion_radius=30.0, threshold=2.0)
+    s = gisspa.Searcher(cfg)
+    s.set_templates(tmpl)
+    picks = s.search(img, ctf)
+    assert len(picks) >= 6
+    INPUTS["norm_l256_w9"] = (img, tmpl, cfg)
+    return s, picks, ctf
+
+
+def test_score_at_pick_equals_search_score(searched):
+    s, picks, ctf = searched
+    g = s.score_grad(picks)
+    assert np.allclose(g["score"], picks["score"], rtol=1e-4, atol=1e-5), (g["score"], picks["score"])
+
+
+def _score(s, picks, params, ctf):
+    return s.score_grad(picks, params, ctf)["score"].astype(np.float64)
+
+
+def test_pick_gradients_match_central_differences(searched):
+    torch = pytest.importorskip("torch")
+    s, picks, ctf = searched
+    picks = picks[:6]
+    base = np.stack([np.full(len(picks), 0.31), np.full(len(picks), -0.23), picks["theta"] + 1.7], 1).astype(np.float32)
+
+    class Score(torch.autograd.Function):
+        """z(dx, dy, theta) of every pick, with the library's adjoint as backward."""
+
+        @staticmethod
+        def forward(ctx, p):
+            g = s.score_grad(picks, p.detach().cpu().numpy().astype(np.float32), ctf)
+            ctx.save_for_backward(torch.from_numpy(np.stack([g["d_dx"], g["d_dy"], g["d_theta"]], 1)))
+            return torch.from_numpy(g["score"].astype(np.float64))
+
+        @staticmethod
+        def backward(ctx, go):
+            (jac,) = ctx.saved_tensors
+            return go[:, None] * jac.to(go.dtype)
+
+    p = torch.tensor(base.astype(np.float64), requires_grad=True)
+    z = Score.apply(p)
+    (adj,) = torch.autograd.grad(z.sum(), p)
+    adj = adj.numpy()
+    fd = np.zeros_like(adj)
+    for k in range(3):
+        d = np.zeros_like(base)
+        d[:, k] = FD_H
+        hi, lo = (base + d).astype(np.float32), (base - d).astype(np.float32)
+        step = hi[:, k].astype(np.float64) - lo[:, k].astype(np.float64)  # the step the float32 ABI sees
+        fd[:, k] = (_score(s, picks, hi, ctf) - _score(s, picks, lo, ctf)) / step
+    for i in range(len(picks)):
+        err = np.linalg.norm(adj[i] - fd[i]) / max(np.linalg.norm(fd[i]), 1e-6)
+        assert err < FD32_RTOL, (i, adj[i], fd[i], err)
+
+
+def test_refine_raises_scores_of_perturbed_picks(searched):
+    s, picks, ctf = searched
+    picks = picks[:8].copy()
+    start = picks.copy()
+    start["x"] += 0.7
+    start["y"] -= 0.6
+    z0 = s.score_grad(picks, np.stack([np.full(len(picks), -0.7), np.full(len(picks), 0.6),
+                                        picks["theta"]], 1).astype(np.float32), ctf)["score"]
+    refined, c2, params = s.refine(picks, steps=20, ctf=None)
+    # refinement starts at the grid picks; it can only move to higher scores
+    assert np.all(refined["score"] >= picks["score"] - 1e-5)
+    assert np.all(refined["score"] >= z0 - 1e-5)
+    # with the CTF refined too, the mean score does not drop
+    refined2, c3, _ = s.refine(picks, steps=10, ctf=gisspa.Ctf(ctf.defocus, ctf.dfdiff, ctf.dfang))
+    assert refined2["score"].mean() >= picks["score"].mean() - 1e-5
+    assert c3 is not None and np.isfinite([c3.defocus, c3.dfdiff, c3.dfang]).all()
+
+
+def test_gradients_match_fp64_oracle(searched):
+    """The library's adjoint against central differences (h = 1e-5, FP64) of the oracle's
+    restatement of the same score."""
+    s, picks, ctf = searched
+    img, tmpl, cfg = INPUTS["norm_l256_w9"]
+    L = cfg.window_size
+    ny, nx = img.shape
+    ox, oy = oracle.window_offsets(nx, L, cfg.overlap), oracle.window_offsets(ny, L, cfg.overlap)
+    bx = len(ox)
+    img_pre = oracle.prep_image(cfg, ctf, img)
+    _, st = oracle.search(cfg, ctf, img, tmpl, want_stats=True)
+    h = 1e-5
+    dfu0, dfv0 = -ctf.defocus + ctf.dfdiff, -ctf.defocus - ctf.dfdiff
+    for p in picks[:3]:
+        b, n = int(p["window"]), int(p["template_id"])
+        px, py = int(p["x"]) - ox[b % bx], int(p["y"]) - oy[b // bx]
+        mu, sd = st[b, py, px]
+        q0 = np.array([0.31, -0.23, float(p["theta"]) + 1.7, dfu0, dfv0, ctf.dfang])
+
+        def f(q):
+            c = gisspa.Ctf(-(q[3] + q[4]) / 2, (q[3] - q[4]) / 2, q[5])
+            prep = oracle.prep_templates(cfg, c, tmpl[n:n + 1])[0].real
+            return oracle.pick_score(cfg, prep, img_pre, (ox[b % bx], oy[b // bx]), px, py, q[0], q[1], q[2], mu, sd)
+
+        g_or = np.zeros(6)
+        for k in range(6):
+            d = np.zeros(6)
+            d[k] = h
+            g_or[k] = (f(q0 + d) - f(q0 - d)) / (2 * h)
+        c0 = gisspa.Ctf(ctf.defocus, ctf.dfdiff, ctf.dfang)
+        g = s.score_grad(p[None], np.array([[q0[0], q0[1], q0[2]]], np.float32), c0)[0]
+        ours = np.array([g["d_dx"], g["d_dy"], g["d_theta"], g["d_dfu"], g["d_dfv"], g["d_dfang"]], np.float64)
+        assert abs(float(g["score"]) - f(q0)) <= 1e-4 * abs(f(q0)) + 1e-5
+        e1 = np.linalg.norm(ours[:3] - g_or[:3]) / max(np.linalg.norm(g_or[:3]), 1e-6)
+        e2 = np.linalg.norm(ours[3:] - g_or[3:]) / max(np.linalg.norm(g_or[3:]), 1e-6)
+        assert e1 < GRAD_RTOL and e2 < GRAD_RTOL, (ours, g_or, e1, e2)
