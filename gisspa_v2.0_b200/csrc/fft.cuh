@@ -91,8 +91,31 @@ __device__ __forceinline__ float2 table_tw(const float2* __restrict__ tw, int p)
   return SIGN > 0 ? make_float2(w.x, -w.y) : w;
 }
 
+// Powers w[m] = w1^m, 1 <= m < R, by products of powers of two: w[2^i] by squaring,
+// w[m] = w[h] w[m - h] with h the highest power of two below m.  The deepest power (m = R - 1)
+// is log2(R) products from w1, so each power carries a few ulp beyond the table entry.
+template <int M, int R>
+struct TwPow {
+  static constexpr int H = M >= 8 ? 8 : M >= 4 ? 4 : M >= 2 ? 2 : 1;  // highest power of two <= M
+  __device__ __forceinline__ static void run(float2* w) {
+    if constexpr (M < R) {
+      w[M] = (H == M) ? cmul(w[M / 2], w[M / 2]) : cmul(w[H], w[M - H]);
+      TwPow<M + 1, R>::run(w);
+    }
+  }
+};
+template <int R>
+__device__ __forceinline__ void tw_powers(float2 w1, float2* w) {
+  static_assert(R <= 16, "powers up to 15");
+  w[1] = w1;
+  TwPow<2, R>::run(w);
+}
+
 // One Stockham stage: v holds this thread's inputs as v[q*R + m] = x[j_q + m N/R].
-// Twiddles, butterflies, and (unless LAST) stores to shared memory.
+// Twiddles, butterflies, and (unless LAST) stores to shared memory.  Each butterfly reads one
+// twiddle W_N^(k step) from the table and raises it to the powers m = 2..R-1 in registers: the
+// table reads are gathers (k varies with the thread), R - 1 per butterfly they took most of the
+// L1 load bandwidth of the correlation passes.
 template <int N, int T, int R, int NS, int SIGN, bool LAST, int S>
 __device__ __forceinline__ void stockham_stage(float2* v, float2* sm, const float2* __restrict__ tw, int tid) {
   constexpr int E = N / T, B = E / R;
@@ -104,8 +127,10 @@ __device__ __forceinline__ void stockham_stage(float2* v, float2* sm, const floa
     float2* a = v + q * R;
     if constexpr (NS > 1) {
       constexpr int step = N / (NS * R);
+      float2 w[R];
+      tw_powers<R>(table_tw<SIGN>(tw, k * step), w);
 #pragma unroll
-      for (int m = 1; m < R; ++m) a[m] = cmul(a[m], table_tw<SIGN>(tw, k * m * step));
+      for (int m = 1; m < R; ++m) a[m] = cmul(a[m], w[m]);
     }
     Dft<R, SIGN>::run(a);
     if constexpr (!LAST) {
