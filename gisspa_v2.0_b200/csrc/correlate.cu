@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
       v[i] = cmulc(__ldg(Ic + ky), SPEC::load(Tc + ky));
     }
   }
-  fft3<L, TT, +1>(v, smem + team * L, twL, tid, BlockSync{});
+  fft3<L, TT, +1>(v, smem + team * L, TwGlobal{twL}, tid, BlockSync{});
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < E; ++i) {
@@ -117,6 +117,13 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   static_assert(RB % NTEAM == 0, "rows must split evenly over teams");
   extern __shared__ __align__(128) float2 stage[];  // [2][RB][NZ]
   __shared__ __align__(8) uint64_t bars[2];
+  // the row transform's table (length NZ) and the first NZ entries of the length-L table
+  // used by the even/odd unpack, staged once: every row of every template reads them
+  __shared__ __align__(16) float2 tw_nz[NZ], tw_l[NZ];
+  for (int i = threadIdx.x; i < NZ; i += NW * 32) {
+    tw_nz[i] = __ldg(twNZ + i);
+    tw_l[i] = __ldg(twL + i);
+  }
   const int team = threadIdx.x / TEAM, lt = threadIdx.x - team * TEAM;
   const int e = blockIdx.y, y0 = blockIdx.x * RB, win = a.b0 + e;
   const float inv = 1.0f / (float)(L * L);
@@ -211,13 +218,13 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         }
         const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
         const float2 od = make_float2(xk.x - xm.x, xk.y + xm.y);
-        float2 w = __ldg(twL + k);
+        float2 w = tw_l[k];
         w.y = -w.y;
         const float2 o = cmul(w, od);
         v[i] = make_float2(ev.x - o.y, ev.y + o.x);
       }
       __syncwarp();
-      fft3<NZ, TEAM, +1>(v, row, twNZ, lt, WarpSync{});
+      fft3<NZ, TEAM, +1>(v, row, TwShared{tw_nz}, lt, WarpSync{});
 
       if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll

@@ -84,10 +84,22 @@ struct Dft {
   }
 };
 
-// Twiddle W_N^p for the stage, from a table of exp(-2 pi i p / N), p < N.
-template <int SIGN>
-__device__ __forceinline__ float2 table_tw(const float2* __restrict__ tw, int p) {
-  float2 w = __ldg(tw + p);
+// Twiddle tables exp(-2 pi i p / N), p < N, read through the read-only path (TwGlobal) or
+// from a copy the CTA staged in shared memory (TwShared, for kernels that sweep the same
+// table many times and would otherwise stall on L1 latency).
+struct TwGlobal {
+  const float2* __restrict__ p;
+  __device__ __forceinline__ float2 operator()(int i) const { return __ldg(p + i); }
+};
+struct TwShared {
+  const float2* p;
+  __device__ __forceinline__ float2 operator()(int i) const { return p[i]; }
+};
+
+// Twiddle W_N^p for the stage (conjugated for the inverse transform).
+template <int SIGN, typename Tw>
+__device__ __forceinline__ float2 table_tw(const Tw& tw, int p) {
+  float2 w = tw(p);
   return SIGN > 0 ? make_float2(w.x, -w.y) : w;
 }
 
@@ -116,8 +128,8 @@ __device__ __forceinline__ void tw_powers(float2 w1, float2* w) {
 // twiddle W_N^(k step) from the table and raises it to the powers m = 2..R-1 in registers: the
 // table reads are gathers (k varies with the thread), R - 1 per butterfly they took most of the
 // L1 load bandwidth of the correlation passes.
-template <int N, int T, int R, int NS, int SIGN, bool LAST, int S>
-__device__ __forceinline__ void stockham_stage(float2* v, float2* sm, const float2* __restrict__ tw, int tid) {
+template <int N, int T, int R, int NS, int SIGN, bool LAST, int S, typename Tw>
+__device__ __forceinline__ void stockham_stage(float2* v, float2* sm, const Tw& tw, int tid) {
   constexpr int E = N / T, B = E / R;
   static_assert(E % R == 0, "radix must divide the points per thread");
 #pragma unroll
@@ -167,8 +179,8 @@ template <> struct Plan<128, 16> { static constexpr int R1 = 8, R2 = 4, R3 = 4, 
 // Full three-stage transform.  v: E inputs in first-stage order; on return v holds
 // the outputs in last-stage order.  sm: this team's buffer of N values; SYNC() must be a
 // barrier covering the team (warp or block).  The buffer is free again on return.
-template <int N, int T, int SIGN, typename Sync>
-__device__ __forceinline__ void fft3(float2* v, float2* sm, const float2* __restrict__ tw, int tid, Sync sync) {
+template <int N, int T, int SIGN, typename Sync, typename Tw>
+__device__ __forceinline__ void fft3(float2* v, float2* sm, const Tw& tw, int tid, Sync sync) {
   using P = Plan<N, T>;
   constexpr int R1 = P::R1, R2 = P::R2, R3 = P::R3, S = P::S;
   static_assert(R1 * R2 * R3 == N, "plan must factor N");
