@@ -50,6 +50,7 @@ void gisspa_config_default(gisspa_config* c) {
   c->pick_mode = GISSPA_PICK_CHUNK; c->topk = 1000; c->exclusion_radius = 64.f;
   c->spectrum_precision = GISSPA_SPEC_FP32; c->template_batch = 0; c->window_batch = 0;
   c->quirks = GISSPA_QUIRKS_REFERENCE; c->tile_size = 720;
+  c->cuda_graphs = 1;
 }
 
 int gisspa_create(const gisspa_config* cfg, int device, gisspa_handle** out) {
@@ -181,6 +182,119 @@ int gisspa_search(gisspa_handle* h, const float* image, int nx, int ny, const gi
   });
   if (st) return st;
   return gisspa_search_device(h, h->img_in.as<float>(), nx, ny, ctf, picks, cap, n_out);
+}
+
+// ---- sharded search (one micrograph across ranks)
+namespace {
+int shard_check(gisspa_handle* h, const char* what, int need_min, int need_max) {
+  if (!h) return GISSPA_ERR_ARG;
+  if (h->cfg.norm_type == 0) {
+    h->err = std::string(what) + ": the sharded search is defined for norm_type=1";
+    return GISSPA_ERR_UNSUPPORTED;
+  }
+  if (h->run.phase < need_min || h->run.phase > need_max) {
+    h->err = std::string(what) + ": called out of order (phase " + std::to_string(h->run.phase) + ")";
+    return GISSPA_ERR_STATE;
+  }
+  return GISSPA_OK;
+}
+}  // namespace
+
+int gisspa_shard_begin(gisspa_handle* h, const float* image, int nx, int ny, const gisspa_ctf* ctf,
+                       gisspa_shard_info* info) {
+  int st = shard_check(h, "shard_begin", 0, 4);
+  if (st) return st;
+  if (!image || !ctf || !info) {
+    h->err = "shard_begin: null argument";
+    return GISSPA_ERR_ARG;
+  }
+  if (!h->templates_ready) {
+    h->err = "shard_begin: gisspa_set_templates has not been called";
+    return GISSPA_ERR_STATE;
+  }
+  st = validate_image(h->cfg, nx, ny, h->err);
+  if (st) return st;
+  h->run.phase = 0;
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    const size_t bytes = sizeof(float) * (size_t)nx * ny;
+    h->img_in.ensure(bytes);
+    GISSPA_CUDA(cudaMemcpyAsync(h->img_in.as<float>(), image, bytes, cudaMemcpyHostToDevice, h->stream));
+    shard_begin(h, h->img_in.as<float>(), nx, ny, *ctf, info);
+  });
+}
+
+int gisspa_shard_sweep(gisspa_handle* h, int sweep, int angle_begin, int angle_end) {
+  if (!h) return GISSPA_ERR_ARG;
+  if (sweep != 1 && sweep != 2) {
+    h->err = "shard_sweep: sweep must be 1 or 2";
+    return GISSPA_ERR_ARG;
+  }
+  int st = sweep == 1 ? shard_check(h, "shard_sweep", 1, 2) : shard_check(h, "shard_sweep", 3, 4);
+  if (st) return st;
+  if (sweep == 2 && h->run.topk) {
+    h->err = "shard_sweep: top-K picking has no second sweep";
+    return GISSPA_ERR_STATE;
+  }
+  const int A = (int)h->run.angles.size();
+  if (angle_begin < 0 || angle_end > A || angle_begin > angle_end) {
+    h->err = "shard_sweep: angle range [" + std::to_string(angle_begin) + ", " + std::to_string(angle_end) +
+             ") outside [0, " + std::to_string(A) + ")";
+    return GISSPA_ERR_ARG;
+  }
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    shard_sweep(h, sweep, angle_begin, angle_end);
+  });
+}
+
+int gisspa_shard_export(gisspa_handle* h, double* sum, double* sum_sq, long long* peak_key) {
+  int st = shard_check(h, "shard_export", 1, 2);
+  if (st) return st;
+  if (!sum || !sum_sq || (h->run.topk && !peak_key)) {
+    h->err = "shard_export: null argument";
+    return GISSPA_ERR_ARG;
+  }
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    shard_export(h, sum, sum_sq, peak_key);
+  });
+}
+
+int gisspa_shard_import(gisspa_handle* h, const double* sum, const double* sum_sq, const long long* peak_key) {
+  int st = shard_check(h, "shard_import", 1, 2);
+  if (st) return st;
+  if (!sum || !sum_sq || (h->run.topk && !peak_key)) {
+    h->err = "shard_import: null argument";
+    return GISSPA_ERR_ARG;
+  }
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    shard_import(h, sum, sum_sq, peak_key);
+  });
+}
+
+int gisspa_shard_picks(gisspa_handle* h, gisspa_pick* picks, size_t cap, size_t* n_out) {
+  if (!h) return GISSPA_ERR_ARG;
+  int st = h->run.topk ? shard_check(h, "shard_picks", 3, 3) : shard_check(h, "shard_picks", 4, 4);
+  if (st) return st;
+  if (!n_out || (cap && !picks)) {
+    h->err = "shard_picks: null argument";
+    return GISSPA_ERR_ARG;
+  }
+  std::vector<gisspa_pick> out;
+  st = guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    shard_picks(h, out);
+  });
+  if (st) return st;
+  *n_out = out.size();
+  if (out.size() > cap) {
+    h->err = "shard_picks: " + std::to_string(out.size()) + " picks exceed capacity " + std::to_string(cap);
+    return GISSPA_ERR_CAPACITY;
+  }
+  if (!out.empty()) std::memcpy(picks, out.data(), sizeof(gisspa_pick) * out.size());
+  return GISSPA_OK;
 }
 
 int gisspa_search_batch(gisspa_handle* h, int n, const float* const* images, const int* nx, const int* ny,

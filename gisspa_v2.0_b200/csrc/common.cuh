@@ -55,6 +55,14 @@ __host__ __device__ __forceinline__ float2 cmul_i(float2 a) {
   return SIGN > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
 
+// Angle of a sweep held in device memory: the rotation and the correlation epilogues read it
+// when given, so one captured CUDA graph of an angle's launches serves every angle.
+struct AngleState {
+  int index;         // position in the float-stepped angle sequence
+  float cose, sine;  // (float)cos / (float)sin of the angle in radians
+  int pad;
+};
+
 // Order-preserving map of a float onto uint32 (larger float -> larger key).
 __device__ __forceinline__ uint32_t float_key(float f) {
   uint32_t b = __float_as_uint(f);

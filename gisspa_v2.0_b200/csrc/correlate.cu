@@ -126,6 +126,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   }
   const int team = threadIdx.x / TEAM, lt = threadIdx.x - team * TEAM;
   const int e = blockIdx.y, y0 = blockIdx.x * RB, win = a.b0 + e;
+  const int angle = a.angle_state ? a.angle_state->index : a.angle;
   const float inv = 1.0f / (float)(L * L);
   const size_t wbase = (size_t)win * L * L;
   if (threadIdx.x == 0) {
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
             if constexpr (EPI == EPI_TOPK) {
               if (c > best[s][i][h]) {
                 best[s][i][h] = c;
-                barg[s][i][h] = a.angle * a.nt_total + a.n0 + d;
+                barg[s][i][h] = angle * a.nt_total + a.n0 + d;
               }
             }
           }
@@ -287,7 +288,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
                     cd.y = py;
                     cd.window = win;
                     cd.templ = a.n0 + d;
-                    cd.angle = a.angle;
+                    cd.angle = angle;
                     cd.chunk = id >> 8;
                     cd.pad = 0;
                     a.cand[slot] = cd;

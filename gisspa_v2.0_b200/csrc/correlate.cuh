@@ -40,6 +40,7 @@ struct CorrArgs {
   int D;                    // templates per window in this launch
   int b0, n0;               // first window / template of the launch
   int angle;                // index of the angle in the angle sequence
+  const AngleState* angle_state;  // when set, the angle index is read here instead (graph replays)
   int nt_real;              // templates >= nt_real never produce picks
   int nt_total;             // N_T used in the (angle, template) combination index
   // EPI_SUM / EPI_TOPK state, [W][L][L]

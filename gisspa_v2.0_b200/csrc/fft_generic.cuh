@@ -6,6 +6,7 @@
 // rows -> transpose -> rows (-> transpose).  All transforms are unnormalised.
 #pragma once
 
+#include <atomic>
 #include <map>
 #include <memory>
 #include <vector>
@@ -13,6 +14,13 @@
 #include "common.cuh"
 
 namespace gisspa {
+
+// Incremented on every device buffer (re)allocation and release in the process: a captured
+// CUDA graph holds raw buffer addresses and is rebuilt when this has moved since its capture.
+inline std::atomic<unsigned long long>& alloc_generation() {
+  static std::atomic<unsigned long long> g{0};
+  return g;
+}
 
 // Grow-only device buffer.
 class DevBuf {
@@ -25,13 +33,17 @@ class DevBuf {
   void* ensure(size_t bytes) {
     if (bytes > n_) {
       release();
+      ++alloc_generation();
       GISSPA_CUDA(cudaMalloc(&p_, bytes));
       n_ = bytes;
     }
     return p_;
   }
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) {
+      ++alloc_generation();
+      cudaFree(p_);
+    }
     p_ = nullptr;
     n_ = 0;
   }

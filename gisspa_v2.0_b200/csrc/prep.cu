@@ -391,8 +391,13 @@ __global__ void gather_windows_kernel(const float* __restrict__ img, int nx, int
 }
 
 __global__ void rotate_kernel(const float* __restrict__ in, int l, float cose, float sine, int mask, float d_m,
-                              float ehw, float2* __restrict__ out, double* __restrict__ sums) {
+                              float ehw, float2* __restrict__ out, double* __restrict__ sums,
+                              const AngleState* __restrict__ st) {
   __shared__ double sh[32];
+  if (st) {
+    cose = st->cose;
+    sine = st->sine;
+  }
   const int n = blockIdx.y;
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   const float* src = in + (size_t)n * l * l;
@@ -559,10 +564,10 @@ void gather_windows(const float* img, int nx, int ny, const int* offx, const int
 }
 
 void rotate_batch(const float* in, int n, int l, float cose, float sine, bool mask, float d_m, float ehw, float2* out,
-                  double* sums, cudaStream_t s) {
+                  double* sums, cudaStream_t s, const AngleState* st) {
   if (sums) GISSPA_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * 2 * n, s));
   rotate_kernel<<<dim3(ceil_div((long long)l * l, kT), n), kT, 0, s>>>(in, l, cose, sine, mask ? 1 : 0, d_m, ehw, out,
-                                                                       sums);
+                                                                       sums, st);
   GISSPA_LAUNCH_CHECK();
 }
 

@@ -51,8 +51,9 @@ void gather_windows(const float* img, int nx, int ny, const int* offx, const int
 
 // ---- rotation (rotate_subIMG kernels.cu:534-603)
 // out[n] = mask(rotate(in[n])) as complex (imag 0); sums[n] = {sum, sum of squares} (FP64)
+// st (optional): read cos/sin from device memory instead of cose/sine (graph replays).
 void rotate_batch(const float* in, int n, int l, float cose, float sine, bool mask, float d_m, float ehw, float2* out,
-                  double* sums, cudaStream_t s);
+                  double* sums, cudaStream_t s, const AngleState* st = nullptr);
 // Write spectra in the kx-major hot layout and storage precision:
 // out[n][kx][ky] = X[n][kx][ky] * scale_n, scale_n = base/sqrt(var_n) when sums are given (and DC = 0:
 // the reference subtracts the mean first), base otherwise.  X is [n][l/2+1][l].

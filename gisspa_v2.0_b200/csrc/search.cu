@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <iterator>
 #include <string>
 #include <vector>
 
@@ -132,6 +133,32 @@ __global__ void fill_kernel(float* __restrict__ a, int* __restrict__ b, long lon
   b[i] = -1;
 }
 
+// Peak keys of the sharded search: ((float_key(c) << 32) | (0xFFFFFFFF - k)) XOR 2^63 as int64,
+// INT64_MIN for a pixel without a correlation (carg < 0).
+__global__ void peak_pack_kernel(const float* __restrict__ cmax, const int* __restrict__ carg, long long n,
+                                 long long* __restrict__ key) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int a = carg[i];
+  unsigned long long k = 0;
+  if (a >= 0) k = ((unsigned long long)float_key(cmax[i]) << 32) | (unsigned)(0xFFFFFFFFu - (unsigned)a);
+  key[i] = (long long)(k ^ 0x8000000000000000ull);
+}
+
+__global__ void peak_unpack_kernel(const long long* __restrict__ key, long long n, float* __restrict__ cmax,
+                                   int* __restrict__ carg) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long k = (unsigned long long)key[i] ^ 0x8000000000000000ull;
+  if (k == 0) {
+    cmax[i] = -INFINITY;
+    carg[i] = -1;
+    return;
+  }
+  cmax[i] = key_float((uint32_t)(k >> 32));
+  carg[i] = (int)(0xFFFFFFFFu - (uint32_t)(k & 0xFFFFFFFFu));
+}
+
 // Top-K: image map of the max z over windows covering each pixel (ties: lowest window).
 __global__ void zmap_kernel(const float* __restrict__ cmax, const int* __restrict__ carg,
                             const float2* __restrict__ ms, int l, const int* __restrict__ offx,
@@ -154,6 +181,15 @@ struct ZCand {
   float z;
   int q, win, arg;
 };
+
+// First node of a captured angle: the angle at the cursor becomes current, the cursor advances.
+__global__ void angle_select_kernel(const AngleState* __restrict__ table, int* __restrict__ cursor,
+                                    AngleState* __restrict__ cur) {
+  *cur = table[*cursor];
+  *cursor += 1;
+}
+
+__global__ void set_int_kernel(int* p, int v) { *p = v; }
 
 __global__ void zcompact_kernel(const unsigned long long* __restrict__ zkey, int nx, int ny, float thresh, float dmin,
                                 const int* __restrict__ carg, int l, const int* __restrict__ offx,
@@ -249,7 +285,8 @@ void window_spectra(Ctx& c, const float* img, int nx, int ny, const std::vector<
 }
 
 // RotateTemplate (norm.cu:479-521): rotate, mask, (x - mean)/sqrt(var), FFT / l^2.
-void template_spectra_at(Ctx& c, float theta) {
+// st (optional): take the angle from device memory (graph replays); theta is then unused.
+void template_spectra_at(Ctx& c, float theta, const AngleState* st = nullptr) {
   gisspa_handle* h = c.h;
   const int l = c.l, nt = h->nt, hs = l / 2 + 1;
   const double rad = (double)theta * kRefPi / 180.0;
@@ -257,7 +294,7 @@ void template_spectra_at(Ctx& c, float theta) {
   float2* rtmp = buf<float2>(h->rot_tmp, (size_t)nt * hs * l);
   double* sums = buf<double>(h->rsums, 2 * (size_t)nt);
   rotate_batch(h->prep_real.as<float>(), nt, l, (float)std::cos(rad), (float)std::sin(rad), true, h->cfg.diameter,
-               h->cfg.edge_half_width, rot, sums, c.s);
+               h->cfg.edge_half_width, rot, sums, c.s, st);
   h->fft.rows(rot, (long long)nt * l, l, -1, 1.f, c.s);
   h->fft.transpose(rot, rtmp, nt, l, l, c.s, hs);
   h->fft.rows(rtmp, (long long)nt * hs, l, -1, 1.f, c.s);
@@ -281,11 +318,13 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   gisspa_handle* h = c.h;
   const int l = c.l;
   struct Cand { int D, E; };
-  std::vector<Cand> cands;
   // (D, E): pass A runs L/2/NC x E CTAs, pass B L/RB x E; Q holds D x E pairs
-  if (l == 512) cands = {{8, 8}, {12, 8}, {6, 12}, {8, 12}, {4, 16}, {6, 16}, {16, 6}, {24, 4}};
-  else if (l == 1024) cands = {{6, 4}, {4, 6}, {3, 8}, {2, 12}, {4, 8}, {8, 3}, {2, 16}};
-  else cands = {{16, 8}, {32, 8}, {8, 16}, {16, 16}, {64, 4}};
+  static const Cand c512[] = {{8, 8}, {12, 8}, {6, 12}, {8, 12}, {4, 16}, {6, 16}, {16, 6}, {24, 4}};
+  static const Cand c1024[] = {{6, 4}, {4, 6}, {3, 8}, {2, 12}, {4, 8}, {8, 3}, {2, 16}};
+  static const Cand c256[] = {{16, 8}, {32, 8}, {8, 16}, {16, 16}, {64, 4}};
+  const Cand* cb = l == 512 ? c512 : l == 1024 ? c1024 : c256;
+  const size_t nc = l == 512 ? std::size(c512) : l == 1024 ? std::size(c1024) : std::size(c256);
+  std::vector<Cand> cands(cb, cb + nc);
   int maxE = 1, maxDE = 1;
   for (auto& cd : cands) {
     cd.D = std::max(1, std::min(cd.D, nt));
@@ -365,7 +404,7 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
       args.n0 = n0;
       args.D = d;
       cudaEvent_t* ev = nullptr;
-      if ((h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples) {
+      if ((h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples && !h->capturing) {
         ev = h->sev[h->n_samples];
         h->sample_pairs[h->n_samples] = d * e;
         h->sample_d[h->n_samples] = d;
@@ -378,11 +417,18 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
   return pairs;
 }
 
-void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_pick>& out) {
+// ---- norm_type = 1 (SearchNorm::work, norm.cu:620-660), in phases.
+
+// Everything before the angle loop: LoadImage statistics, templates, micrograph, windows, the
+// zeroed per-pixel state and the launch shape.
+void norm_prepare(Ctx& c, const float* d_img, int nx, int ny, NormRun& r) {
   gisspa_handle* h = c.h;
   const gisspa_config& cfg = h->cfg;
   const int l = c.l, nt = h->nt;
-  const long long N = (long long)nx * ny;
+  r = NormRun{};
+  r.nx = nx;
+  r.ny = ny;
+  r.N = (long long)nx * ny;
   GISSPA_CUDA(cudaEventRecord(h->ev[0], c.s));
   // LoadImage statistics on the side stream (the serial FP32 form occupies one SM for
   // ~4 ns per pixel) while the templates are prepared on the main stream
@@ -395,186 +441,337 @@ void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_
   prepare_templates(c);
   GISSPA_CUDA(cudaStreamWaitEvent(c.s, h->ev_stats, 0));
   // micrograph
-  float2* G = buf<float2>(h->img_c, N);
-  image_load(d_img, N, stats, true, cfg.invert != 0, G, c.s);
+  float2* G = buf<float2>(h->img_c, r.N);
+  image_load(d_img, r.N, stats, true, cfg.invert != 0, G, c.s);
   preprocess_full(c, G, nx, ny, true);
-  float* img = buf<float>(h->img_pre, N);
-  real_part(G, img, N, 1.f, c.s);
-  const std::vector<int> ox = window_offsets(nx, l, cfg.overlap), oy = window_offsets(ny, l, cfg.overlap);
-  const int bx = (int)ox.size(), W = bx * (int)oy.size();
-  window_spectra(c, img, nx, ny, ox, oy);
+  float* img = buf<float>(h->img_pre, r.N);
+  real_part(G, img, r.N, 1.f, c.s);
+  r.ox = window_offsets(nx, l, cfg.overlap);
+  r.oy = window_offsets(ny, l, cfg.overlap);
+  r.bx = (int)r.ox.size();
+  r.W = r.bx * (int)r.oy.size();
+  window_spectra(c, img, nx, ny, r.ox, r.oy);
   GISSPA_CUDA(cudaEventRecord(h->ev[1], c.s));
   h->last_nx = nx;
   h->last_ny = ny;
-  h->last_W = W;
-  h->last_bx = bx;
-  h->last_offx = ox;
-  h->last_offy = oy;
+  h->last_W = r.W;
+  h->last_bx = r.bx;
+  h->last_offx = r.ox;
+  h->last_offy = r.oy;
 
-  const std::vector<float> angles = angle_list(cfg.phistep);
-  h->last_angles = angles;
-  const int n_euler = (cfg.quirks & GISSPA_QUIRK_NEULER_TRUNC) ? (int)(360.0f / cfg.phistep) : (int)angles.size();
-  const int batch = (cfg.quirks & GISSPA_QUIRK_COUNT_PADDED_TEMPLATES) ? std::max(nt, W) : nt;
-  const double Ntot = (double)batch * n_euler;
-  const bool topk = cfg.pick_mode == GISSPA_PICK_TOPK;
-  const size_t npix = (size_t)W * c.L2;
-  double* S1 = buf<double>(h->S1, npix);
-  double* S2 = buf<double>(h->S2, npix);
-  GISSPA_CUDA(cudaMemsetAsync(S1, 0, sizeof(double) * npix, c.s));
-  GISSPA_CUDA(cudaMemsetAsync(S2, 0, sizeof(double) * npix, c.s));
-  CorrArgs args{};
+  r.angles = angle_list(cfg.phistep);
+  h->last_angles = r.angles;
+  const int n_euler =
+      (cfg.quirks & GISSPA_QUIRK_NEULER_TRUNC) ? (int)(360.0f / cfg.phistep) : (int)r.angles.size();
+  const int batch = (cfg.quirks & GISSPA_QUIRK_COUNT_PADDED_TEMPLATES) ? std::max(nt, r.W) : nt;
+  r.Ntot = (double)batch * n_euler;
+  r.topk = cfg.pick_mode == GISSPA_PICK_TOPK;
+  r.npix = (size_t)r.W * c.L2;
+  double* S1 = buf<double>(h->S1, r.npix);
+  double* S2 = buf<double>(h->S2, r.npix);
+  GISSPA_CUDA(cudaMemsetAsync(S1, 0, sizeof(double) * r.npix, c.s));
+  GISSPA_CUDA(cudaMemsetAsync(S2, 0, sizeof(double) * r.npix, c.s));
+  CorrArgs& args = r.args;
   args.S1 = S1;
   args.S2 = S2;
   args.nt_real = nt;
   args.nt_total = nt;
   args.offx = h->offx.as<int>();
   args.offy = h->offy.as<int>();
-  args.bx = bx;
+  args.bx = r.bx;
   args.nx = nx;
   args.ny = ny;
   args.dmin = cfg.diameter;
   args.thresh = cfg.threshold;
-  if (topk) {
-    args.cmax = buf<float>(h->cmax, npix);
-    args.carg = buf<int>(h->carg, npix);
-    fill_kernel<<<ceil_div((long long)npix, 256), 256, 0, c.s>>>(args.cmax, args.carg, (long long)npix);
+  if (r.topk) {
+    args.cmax = buf<float>(h->cmax, r.npix);
+    args.carg = buf<int>(h->carg, r.npix);
+    fill_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, c.s>>>(args.cmax, args.carg, (long long)r.npix);
     GISSPA_LAUNCH_CHECK();
   }
-  int D, E;
-  choose_batches(cfg, l, W, nt, D, E);
-  const void* T = nullptr;
-  long long pairs = 0;
-  // sweep 1 (ComputeCCGSum norm.cu:523-544), or the single top-K sweep
-  for (size_t a = 0; a < angles.size(); ++a) {
-    template_spectra_at(c, angles[a]);
-    T = h->tspec.as<void>();
-    args.angle = (int)a;
-    pairs += correlate_all(c, topk ? EPI_TOPK : EPI_SUM, h->ispec.as<float2>(), W, T, nt, args, D, E);
-  }
-  float2* ms = buf<float2>(h->musig, npix);
-  musig_kernel<<<ceil_div((long long)npix, 256), 256, 0, c.s>>>(S1, S2, (long long)npix, Ntot, ms);
-  GISSPA_LAUNCH_CHECK();
-  GISSPA_CUDA(cudaEventRecord(h->ev[2], c.s));
-  args.musig = ms;
+  choose_batches(cfg, l, r.W, nt, r.D, r.E);
+  r.phase = 1;
+}
 
-  if (!topk) {
-    // sweep 2 (PickParticles norm.cu:554-600)
-    unsigned cap = (unsigned)std::max<size_t>(h->cand.size() / sizeof(Cand), 1u << 16);
-    for (int attempt = 0; attempt < 2; ++attempt) {
-      Cand* cand = buf<Cand>(h->cand, cap);
-      unsigned* cnt = buf<unsigned>(h->cand_count, 1);
-      GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
-      args.cand = cand;
-      args.cand_count = cnt;
-      args.cand_cap = cap;
-      for (size_t a = 0; a < angles.size(); ++a) {
-        template_spectra_at(c, angles[a]);
-        args.angle = (int)a;
-        pairs += correlate_all(c, EPI_CHUNK, h->ispec.as<float2>(), W, h->tspec.as<void>(), nt, args, D, E);
-      }
-      GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
-      unsigned count = 0;
-      GISSPA_CUDA(cudaMemcpyAsync(&count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c.s));
-      GISSPA_CUDA(cudaStreamSynchronize(c.s));
-      h->st.candidates = count;
-      if (count > cap) {  // grow and repeat the second sweep only
-        cap = count + count / 4 + 1024;
-        continue;
-      }
-      std::vector<Cand> hc(count);
-      if (count)
-        GISSPA_CUDA(cudaMemcpyAsync(hc.data(), cand, sizeof(Cand) * count, cudaMemcpyDeviceToHost, c.s));
-      GISSPA_CUDA(cudaStreamSynchronize(c.s));
-      // reference output order: angle, window (j outer, i inner), template, chunk (norm.cu:561-598)
-      std::sort(hc.begin(), hc.end(), [](const Cand& u, const Cand& v) {
-        if (u.angle != v.angle) return u.angle < v.angle;
-        if (u.window != v.window) return u.window < v.window;
-        if (u.templ != v.templ) return u.templ < v.templ;
-        return u.chunk < v.chunk;
-      });
-      out.reserve(hc.size());
-      for (const Cand& cd : hc) {
-        gisspa_pick pk{};
-        pk.score = cd.score;
-        pk.x = (float)(ox[cd.window % bx] + cd.x);
-        pk.y = (float)(oy[cd.window / bx] + cd.y);
-        float cur_e = 360.0f - angles[cd.angle];  // norm.cu:700-701
-        if (cur_e >= 360.0f) cur_e -= 360.0f;
-        pk.angle = cur_e;
-        pk.theta = angles[cd.angle];
-        pk.template_id = cd.templ;
-        pk.window = cd.window;
-        pk.tile = 0;
-        pk.angle_index = cd.angle;
-        pk.chunk = cd.chunk;
-        out.push_back(pk);
-      }
-      break;
-    }
-  } else {
-    unsigned long long* zk = buf<unsigned long long>(h->zkey, N);
-    GISSPA_CUDA(cudaMemsetAsync(zk, 0, sizeof(unsigned long long) * N, c.s));
-    zmap_kernel<<<dim3(ceil_div(c.L2, 256), W), 256, 0, c.s>>>(args.cmax, args.carg, ms, l, args.offx, args.offy, bx,
-                                                                nx, ny, zk);
-    GISSPA_LAUNCH_CHECK();
-    unsigned cap = (unsigned)std::max<size_t>(h->zcand.size() / sizeof(ZCand), 1u << 16);
-    std::vector<ZCand> hz;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-      ZCand* zc = buf<ZCand>(h->zcand, cap);
-      unsigned* cnt = buf<unsigned>(h->zcount, 1);
-      GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
-      zcompact_kernel<<<ceil_div(N, 256), 256, 0, c.s>>>(zk, nx, ny, cfg.threshold, cfg.diameter, args.carg, l,
-                                                          args.offx, args.offy, bx, zc, cnt, cap);
-      GISSPA_LAUNCH_CHECK();
-      unsigned count = 0;
-      GISSPA_CUDA(cudaMemcpyAsync(&count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c.s));
-      GISSPA_CUDA(cudaStreamSynchronize(c.s));
-      if (count > cap) {
-        cap = count + 1024;
-        continue;
-      }
-      hz.resize(count);
-      if (count) GISSPA_CUDA(cudaMemcpy(hz.data(), zc, sizeof(ZCand) * count, cudaMemcpyDeviceToHost));
-      break;
-    }
-    GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
-    h->st.candidates = (long long)hz.size();
-    std::sort(hz.begin(), hz.end(), [](const ZCand& u, const ZCand& v) {
-      if (u.z != v.z) return u.z > v.z;
-      return u.q < v.q;
-    });
-    const double r2 = (double)cfg.exclusion_radius * cfg.exclusion_radius;
-    std::vector<int> acc;
-    for (const ZCand& zc : hz) {
-      if ((int)acc.size() >= cfg.topk) break;
-      const int x = zc.q % nx, y = zc.q / nx;
-      bool ok = true;
-      for (int q2 : acc) {
-        const double dx = x - q2 % nx, dy = y - q2 / nx;
-        if (dx * dx + dy * dy <= r2) {
-          ok = false;
-          break;
-        }
-      }
-      if (!ok) continue;
-      acc.push_back(zc.q);
-      gisspa_pick pk{};
-      pk.score = zc.z;
-      pk.x = (float)x;
-      pk.y = (float)y;
-      const int a = zc.arg / nt, n = zc.arg % nt;
-      float cur_e = 360.0f - angles[a];
-      if (cur_e >= 360.0f) cur_e -= 360.0f;
-      pk.angle = cur_e;
-      pk.theta = angles[a];
-      pk.template_id = n;
-      pk.window = zc.win;
-      pk.angle_index = a;
-      pk.chunk = (int)acc.size() - 1;
-      out.push_back(pk);
+template <typename T>
+void key_put(std::vector<unsigned char>& k, const T& v) {
+  const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), p, p + sizeof(T));
+}
+
+// Everything one captured angle depends on besides the angle: shapes, buffer addresses, and the
+// epilogue's arguments (device contents such as window offsets are read at replay time).
+std::vector<unsigned char> angle_graph_key(Ctx& c, const NormRun& r, int epi) {
+  gisspa_handle* h = c.h;
+  const CorrArgs& a = r.args;
+  std::vector<unsigned char> k;
+  for (int v : {epi, c.l, r.W, h->nt, r.D, r.E, h->cfg.spectrum_precision, a.nt_real, a.nt_total, a.bx, a.nx, a.ny})
+    key_put(k, v);
+  for (float v : {a.thresh, a.dmin, h->cfg.diameter, h->cfg.edge_half_width}) key_put(k, v);
+  key_put(k, a.cand_cap);
+  for (const void* p : {(const void*)h->prep_real.as<void>(), (const void*)h->rot.as<void>(),
+                        (const void*)h->rot_tmp.as<void>(), (const void*)h->rsums.as<void>(),
+                        (const void*)h->tspec.as<void>(), (const void*)h->ispec.as<void>(),
+                        (const void*)h->Q.as<void>(), (const void*)a.S1, (const void*)a.S2, (const void*)a.cmax,
+                        (const void*)a.carg, (const void*)a.musig, (const void*)a.offx, (const void*)a.offy,
+                        (const void*)a.cand, (const void*)a.cand_count, (const void*)h->dev_err.as<void>(),
+                        (const void*)h->angle_table.as<void>(), (const void*)h->angle_cursor.as<void>(),
+                        (const void*)h->angle_cur.as<void>()})
+    key_put(k, p);
+  return k;
+}
+
+// The captured graph of one angle of this sweep (captured on first use, and again whenever its
+// key changes or any device buffer has been reallocated since).
+AngleGraph& angle_graph(Ctx& c, NormRun& r, int epi) {
+  gisspa_handle* h = c.h;
+  std::vector<unsigned char> key = angle_graph_key(c, r, epi);
+  const unsigned long long gen = alloc_generation().load();
+  for (auto it = h->graphs.begin(); it != h->graphs.end();) {
+    if (it->generation != gen) {  // stale addresses: never replay again
+      cudaGraphExecDestroy(it->exec);
+      it = h->graphs.erase(it);
+    } else if (it->key == key) {
+      return *it;
+    } else {
+      ++it;
     }
   }
-  h->st.pairs = pairs;
+  if (h->graphs.size() >= 8) {
+    cudaGraphExecDestroy(h->graphs.front().exec);
+    h->graphs.erase(h->graphs.begin());
+  }
+  AngleState* cur = h->angle_cur.as<AngleState>();
+  r.args.angle_state = cur;
+  const long long l0 = launch_counter();
+  cudaGraph_t graph = nullptr;
+  long long pairs = 0;
+  h->capturing = true;
+  GISSPA_CUDA(cudaStreamBeginCapture(c.s, cudaStreamCaptureModeThreadLocal));
+  try {
+    angle_select_kernel<<<1, 1, 0, c.s>>>(h->angle_table.as<AngleState>(), h->angle_cursor.as<int>(), cur);
+    GISSPA_LAUNCH_CHECK();
+    template_spectra_at(c, 0.f, cur);
+    pairs = correlate_all(c, epi, h->ispec.as<float2>(), r.W, h->tspec.as<void>(), h->nt, r.args, r.D, r.E);
+  } catch (...) {
+    h->capturing = false;
+    r.args.angle_state = nullptr;
+    cudaStreamEndCapture(c.s, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    throw;
+  }
+  h->capturing = false;
+  r.args.angle_state = nullptr;
+  GISSPA_CUDA(cudaStreamEndCapture(c.s, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  GISSPA_CUDA(e);
+  AngleGraph g;
+  g.key = std::move(key);
+  g.generation = gen;
+  g.exec = exec;
+  g.launches = launch_counter() - l0;
+  g.pairs = pairs;
+  launch_counter() = l0;  // the captured kernels run, and are counted, at each replay
+  h->graphs.push_back(std::move(g));
+  return h->graphs.back();
+}
+
+// Angles [a0, a1) of one sweep.  With cuda_graphs, the first angle runs from the host (it
+// allocates, autotunes and samples the pass timings) and the rest replay one captured graph.
+void run_angles(Ctx& c, NormRun& r, int epi, int a0, int a1) {
+  gisspa_handle* h = c.h;
+  const bool graphs = h->cfg.cuda_graphs != 0 && a1 - a0 >= 3;
+  for (int a = a0; a < (graphs ? a0 + 1 : a1); ++a) {
+    template_spectra_at(c, r.angles[a]);
+    r.args.angle = a;
+    r.args.angle_state = nullptr;
+    r.pairs += correlate_all(c, epi, h->ispec.as<float2>(), r.W, h->tspec.as<void>(), h->nt, r.args, r.D, r.E);
+  }
+  if (!graphs) return;
+  AngleState* table = buf<AngleState>(h->angle_table, r.angles.size());
+  int* cursor = buf<int>(h->angle_cursor, 1);
+  buf<AngleState>(h->angle_cur, 1);
+  if (!r.angle_table_ready) {
+    std::vector<AngleState>& t = r.angle_table;
+    t.resize(r.angles.size());
+    for (size_t a = 0; a < t.size(); ++a) {
+      const double rad = (double)r.angles[a] * kRefPi / 180.0;  // as template_spectra_at
+      t[a] = AngleState{(int)a, (float)std::cos(rad), (float)std::sin(rad), 0};
+    }
+    GISSPA_CUDA(cudaMemcpyAsync(table, t.data(), sizeof(AngleState) * t.size(), cudaMemcpyHostToDevice, c.s));
+    r.angle_table_ready = true;
+  }
+  set_int_kernel<<<1, 1, 0, c.s>>>(cursor, a0 + 1);
+  GISSPA_LAUNCH_CHECK();
+  AngleGraph& g = angle_graph(c, r, epi);
+  for (int a = a0 + 1; a < a1; ++a) GISSPA_CUDA(cudaGraphLaunch(g.exec, c.s));
+  launch_counter() += g.launches * (a1 - a0 - 1);
+  r.pairs += g.pairs * (a1 - a0 - 1);
+  h->graph_replays += a1 - a0 - 1;
+}
+
+// Sweep 1 (ComputeCCGSum norm.cu:523-544) or the single top-K sweep over angles [a0, a1).
+void norm_sweep1(Ctx& c, NormRun& r, int a0, int a1) {
+  run_angles(c, r, r.topk ? EPI_TOPK : EPI_SUM, a0, a1);
+  r.phase = 2;
+}
+
+// set_CCG_mean (kernels.cu:697-706): mu and 1/sigma per window pixel from the complete sums.
+void norm_stats(Ctx& c, NormRun& r) {
+  float2* ms = buf<float2>(c.h->musig, r.npix);
+  musig_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, c.s>>>(r.args.S1, r.args.S2, (long long)r.npix, r.Ntot,
+                                                                    ms);
+  GISSPA_LAUNCH_CHECK();
+  r.args.musig = ms;
+  r.phase = 3;
+}
+
+// Sweep 2 (PickParticles norm.cu:554-600) over angles [a0, a1): chunk candidates, grown and
+// repeated once when the buffer overflows, left in r.cand in the reference's output order
+// (angle, window with j outer and i inner, template, chunk; norm.cu:561-598).
+void norm_sweep2(Ctx& c, NormRun& r, int a0, int a1) {
+  gisspa_handle* h = c.h;
+  unsigned cap = (unsigned)std::max<size_t>(h->cand.size() / sizeof(Cand), 1u << 16);
+  r.cand.clear();
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    Cand* cand = buf<Cand>(h->cand, cap);
+    unsigned* cnt = buf<unsigned>(h->cand_count, 1);
+    GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
+    r.args.cand = cand;
+    r.args.cand_count = cnt;
+    r.args.cand_cap = cap;
+    run_angles(c, r, EPI_CHUNK, a0, a1);
+    GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
+    unsigned count = 0;
+    GISSPA_CUDA(cudaMemcpyAsync(&count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c.s));
+    GISSPA_CUDA(cudaStreamSynchronize(c.s));
+    h->st.candidates = count;
+    if (count > cap) {  // grow and repeat the second sweep only
+      cap = count + count / 4 + 1024;
+      continue;
+    }
+    r.cand.resize(count);
+    if (count) GISSPA_CUDA(cudaMemcpyAsync(r.cand.data(), cand, sizeof(Cand) * count, cudaMemcpyDeviceToHost, c.s));
+    GISSPA_CUDA(cudaStreamSynchronize(c.s));
+    std::sort(r.cand.begin(), r.cand.end(), [](const Cand& u, const Cand& v) {
+      if (u.angle != v.angle) return u.angle < v.angle;
+      if (u.window != v.window) return u.window < v.window;
+      if (u.templ != v.templ) return u.templ < v.templ;
+      return u.chunk < v.chunk;
+    });
+    break;
+  }
+  r.phase = 4;
+}
+
+void chunk_picks(const NormRun& r, std::vector<gisspa_pick>& out) {
+  out.reserve(out.size() + r.cand.size());
+  for (const Cand& cd : r.cand) {
+    gisspa_pick pk{};
+    pk.score = cd.score;
+    pk.x = (float)(r.ox[cd.window % r.bx] + cd.x);
+    pk.y = (float)(r.oy[cd.window / r.bx] + cd.y);
+    float cur_e = 360.0f - r.angles[cd.angle];  // norm.cu:700-701
+    if (cur_e >= 360.0f) cur_e -= 360.0f;
+    pk.angle = cur_e;
+    pk.theta = r.angles[cd.angle];
+    pk.template_id = cd.templ;
+    pk.window = cd.window;
+    pk.tile = 0;
+    pk.angle_index = cd.angle;
+    pk.chunk = cd.chunk;
+    out.push_back(pk);
+  }
+}
+
+// Top-K on the image map of the max z: threshold, centre rule, greedy exclusion in score order.
+void topk_picks(Ctx& c, NormRun& r, std::vector<gisspa_pick>& out) {
+  gisspa_handle* h = c.h;
+  const gisspa_config& cfg = h->cfg;
+  const int l = c.l, nt = h->nt, nx = r.nx, ny = r.ny, bx = r.bx;
+  const long long N = r.N;
+  unsigned long long* zk = buf<unsigned long long>(h->zkey, N);
+  GISSPA_CUDA(cudaMemsetAsync(zk, 0, sizeof(unsigned long long) * N, c.s));
+  zmap_kernel<<<dim3(ceil_div(c.L2, 256), r.W), 256, 0, c.s>>>(r.args.cmax, r.args.carg, r.args.musig, l, r.args.offx,
+                                                                r.args.offy, bx, nx, ny, zk);
+  GISSPA_LAUNCH_CHECK();
+  unsigned cap = (unsigned)std::max<size_t>(h->zcand.size() / sizeof(ZCand), 1u << 16);
+  std::vector<ZCand> hz;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    ZCand* zc = buf<ZCand>(h->zcand, cap);
+    unsigned* cnt = buf<unsigned>(h->zcount, 1);
+    GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
+    zcompact_kernel<<<ceil_div(N, 256), 256, 0, c.s>>>(zk, nx, ny, cfg.threshold, cfg.diameter, r.args.carg, l,
+                                                        r.args.offx, r.args.offy, bx, zc, cnt, cap);
+    GISSPA_LAUNCH_CHECK();
+    unsigned count = 0;
+    GISSPA_CUDA(cudaMemcpyAsync(&count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c.s));
+    GISSPA_CUDA(cudaStreamSynchronize(c.s));
+    if (count > cap) {
+      cap = count + 1024;
+      continue;
+    }
+    hz.resize(count);
+    if (count) GISSPA_CUDA(cudaMemcpy(hz.data(), zc, sizeof(ZCand) * count, cudaMemcpyDeviceToHost));
+    break;
+  }
+  GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
+  h->st.candidates = (long long)hz.size();
+  std::sort(hz.begin(), hz.end(), [](const ZCand& u, const ZCand& v) {
+    if (u.z != v.z) return u.z > v.z;
+    return u.q < v.q;
+  });
+  const double r2 = (double)cfg.exclusion_radius * cfg.exclusion_radius;
+  std::vector<int> acc;
+  for (const ZCand& zc : hz) {
+    if ((int)acc.size() >= cfg.topk) break;
+    const int x = zc.q % nx, y = zc.q / nx;
+    bool ok = true;
+    for (int q2 : acc) {
+      const double dx = x - q2 % nx, dy = y - q2 / nx;
+      if (dx * dx + dy * dy <= r2) {
+        ok = false;
+        break;
+      }
+    }
+    if (!ok) continue;
+    acc.push_back(zc.q);
+    gisspa_pick pk{};
+    pk.score = zc.z;
+    pk.x = (float)x;
+    pk.y = (float)y;
+    const int a = zc.arg / nt, n = zc.arg % nt;
+    float cur_e = 360.0f - r.angles[a];
+    if (cur_e >= 360.0f) cur_e -= 360.0f;
+    pk.angle = cur_e;
+    pk.theta = r.angles[a];
+    pk.template_id = n;
+    pk.window = zc.win;
+    pk.angle_index = a;
+    pk.chunk = (int)acc.size() - 1;
+    out.push_back(pk);
+  }
+}
+
+void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_pick>& out) {
+  gisspa_handle* h = c.h;
+  NormRun& r = h->run;
+  norm_prepare(c, d_img, nx, ny, r);
+  const int A = (int)r.angles.size();
+  norm_sweep1(c, r, 0, A);
+  norm_stats(c, r);
+  GISSPA_CUDA(cudaEventRecord(h->ev[2], c.s));
+  if (!r.topk) {
+    norm_sweep2(c, r, 0, A);
+    chunk_picks(r, out);
+  } else {
+    topk_picks(c, r, out);
+  }
+  h->st.pairs = r.pairs;
+  r.phase = 0;
 }
 
 // norm_type = 0 (SearchNoNorm, nonorm.cu): 720^2 tiles, rotate the windows, per-template best.
@@ -1038,6 +1235,88 @@ void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const giss
     h->st.templates_per_launch = dd / h->n_samples;
   }
   h->st.pass_samples = h->n_samples;
+}
+
+// ---- sharded norm_type=1 search: one contiguous angle range per rank, state merged by the
+// caller's collective between the phases.
+namespace {
+Ctx shard_ctx(gisspa_handle* h) {
+  return Ctx{h, h->stream, h->cfg.window_size, (long long)h->cfg.window_size * h->cfg.window_size,
+             make_params(h->cfg, h->last_ctf)};
+}
+
+void shard_sync(gisspa_handle* h, const char* where) {
+  GISSPA_CUDA(cudaStreamSynchronize(h->stream));
+  unsigned flag = 0;
+  GISSPA_CUDA(cudaMemcpy(&flag, h->dev_err.as<unsigned>(), sizeof(flag), cudaMemcpyDeviceToHost));
+  if (flag) throw TimeoutError{where};
+}
+}  // namespace
+
+void shard_begin(gisspa_handle* h, const float* d_img, int nx, int ny, const gisspa_ctf& ctf,
+                 gisspa_shard_info* info) {
+  h->last_ctf = ctf;
+  h->last_W = 0;
+  h->st = gisspa_stats{};
+  h->n_samples = 0;
+  h->launch_index = 0;
+  Ctx c = shard_ctx(h);
+  unsigned* err = buf<unsigned>(h->dev_err, 1);
+  GISSPA_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), c.s));
+  norm_prepare(c, d_img, nx, ny, h->run);
+  shard_sync(h, "shard_begin");
+  info->n_pixels = h->run.npix;
+  info->n_windows = h->run.W;
+  info->n_angles = (int)h->run.angles.size();
+  info->pick_mode = h->cfg.pick_mode;
+}
+
+void shard_sweep(gisspa_handle* h, int sweep, int a0, int a1) {
+  Ctx c = shard_ctx(h);
+  NormRun& r = h->run;
+  if (sweep == 1)
+    norm_sweep1(c, r, a0, a1);
+  else
+    norm_sweep2(c, r, a0, a1);
+  h->st.pairs = r.pairs;
+  shard_sync(h, "shard_sweep");
+}
+
+void shard_export(gisspa_handle* h, double* sum, double* sum_sq, long long* peak_key) {
+  NormRun& r = h->run;
+  cudaStream_t s = h->stream;
+  GISSPA_CUDA(cudaMemcpyAsync(sum, r.args.S1, sizeof(double) * r.npix, cudaMemcpyDeviceToDevice, s));
+  GISSPA_CUDA(cudaMemcpyAsync(sum_sq, r.args.S2, sizeof(double) * r.npix, cudaMemcpyDeviceToDevice, s));
+  if (r.topk && peak_key) {
+    peak_pack_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, s>>>(r.args.cmax, r.args.carg, (long long)r.npix,
+                                                                       peak_key);
+    GISSPA_LAUNCH_CHECK();
+  }
+  shard_sync(h, "shard_export");
+}
+
+void shard_import(gisspa_handle* h, const double* sum, const double* sum_sq, const long long* peak_key) {
+  Ctx c = shard_ctx(h);
+  NormRun& r = h->run;
+  GISSPA_CUDA(cudaMemcpyAsync(r.args.S1, sum, sizeof(double) * r.npix, cudaMemcpyDeviceToDevice, c.s));
+  GISSPA_CUDA(cudaMemcpyAsync(r.args.S2, sum_sq, sizeof(double) * r.npix, cudaMemcpyDeviceToDevice, c.s));
+  if (r.topk) {
+    peak_unpack_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, c.s>>>(peak_key, (long long)r.npix, r.args.cmax,
+                                                                           r.args.carg);
+    GISSPA_LAUNCH_CHECK();
+  }
+  norm_stats(c, r);
+  shard_sync(h, "shard_import");
+}
+
+void shard_picks(gisspa_handle* h, std::vector<gisspa_pick>& out) {
+  Ctx c = shard_ctx(h);
+  NormRun& r = h->run;
+  if (r.topk)
+    topk_picks(c, r, out);
+  else
+    chunk_picks(r, out);
+  shard_sync(h, "shard_picks");
 }
 
 int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx, const int* ny,

@@ -8,6 +8,7 @@
 
 #include "../../include/gisspa.h"
 #include "common.cuh"
+#include "correlate.cuh"
 #include "fft_generic.cuh"
 
 namespace gisspa {
@@ -15,6 +16,36 @@ namespace gisspa {
 struct TuneChoice {
   int variant = 0, D = 1, E = 1;
   double us_per_pair = 0;
+};
+
+// One norm_type=1 search between its phases: preparation, sweeps over angle ranges, the
+// normalisation statistics, picks.  Kept in the handle so that the sharded entry points
+// (one angle range per rank, state merged by the caller's collective) can resume it.
+struct NormRun {
+  int phase = 0;  // 0 none, 1 prepared, 2 sweep 1 done (this rank's range), 3 statistics in place,
+                  // 4 sweep 2 done
+  int nx = 0, ny = 0, W = 0, bx = 0;
+  long long N = 0;
+  size_t npix = 0;
+  std::vector<int> ox, oy;
+  std::vector<float> angles;
+  double Ntot = 0;
+  bool topk = false;
+  int D = 1, E = 1;
+  CorrArgs args{};
+  long long pairs = 0;
+  std::vector<Cand> cand;  // sweep 2 candidates of the last range, reference order
+  bool angle_table_ready = false;
+  std::vector<AngleState> angle_table;  // host copy, alive while its upload is in flight
+};
+
+// One angle's launches of a sweep captured as a CUDA graph: the angle comes from a device
+// cursor advanced by the graph's first node, so replaying it walks the angle sequence.
+struct AngleGraph {
+  std::vector<unsigned char> key;   // shapes, buffer addresses and epilogue arguments captured
+  unsigned long long generation = 0;  // alloc_generation() at capture
+  cudaGraphExec_t exec = nullptr;
+  long long launches = 0, pairs = 0;  // kernels and (window, template) pairs per replay
 };
 }  // namespace gisspa
 
@@ -56,6 +87,12 @@ struct gisspa_handle {
   gisspa_ctf last_ctf{};
   std::vector<int> last_offx, last_offy;
   std::vector<float> last_angles;
+  gisspa::NormRun run;  // the norm_type=1 search in progress (sharded entry points)
+  // CUDA-graph replay of the sweeps' angles
+  std::vector<gisspa::AngleGraph> graphs;
+  gisspa::DevBuf angle_table, angle_cursor, angle_cur;
+  bool capturing = false;
+  long long graph_replays = 0;
 
   gisspa_stats st{};
   std::map<long long, gisspa::TuneChoice> tuned;
@@ -68,6 +105,8 @@ struct gisspa_handle {
   long long launch_index = 0;
 
   ~gisspa_handle() {
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     for (auto& r : sev)
@@ -111,6 +150,13 @@ int guarded(gisspa_handle* h, F&& fn) {
 
 void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const gisspa_ctf& ctf,
                 std::vector<gisspa_pick>& out);
+// Sharded norm_type=1 search (see gisspa_shard_* in gisspa.h).
+void shard_begin(gisspa_handle* h, const float* d_img, int nx, int ny, const gisspa_ctf& ctf,
+                 gisspa_shard_info* info);
+void shard_sweep(gisspa_handle* h, int sweep, int a0, int a1);
+void shard_export(gisspa_handle* h, double* sum, double* sum_sq, long long* peak_key);
+void shard_import(gisspa_handle* h, const double* sum, const double* sum_sq, const long long* peak_key);
+void shard_picks(gisspa_handle* h, std::vector<gisspa_pick>& out);
 int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx, const int* ny,
               const gisspa_ctf* ctfs, gisspa_pick* picks, size_t cap, size_t* offsets);
 

@@ -38,7 +38,7 @@ class Config(C.Structure):
                                          "bfactor3")] + \
                [("pick_mode", C.c_int), ("topk", C.c_int), ("exclusion_radius", C.c_float),
                 ("spectrum_precision", C.c_int), ("template_batch", C.c_int), ("window_batch", C.c_int),
-                ("quirks", C.c_int), ("tile_size", C.c_int)]
+                ("quirks", C.c_int), ("tile_size", C.c_int), ("cuda_graphs", C.c_int)]
 
     @classmethod
     def default(cls, **kw) -> "Config":
@@ -51,7 +51,7 @@ class Config(C.Structure):
         c.a, c.b, c.b2, c.bfactor, c.bfactor2, c.bfactor3 = -10.81, 1.0, 0.32, -18.17, -15.22, 1.72
         c.pick_mode, c.topk, c.exclusion_radius = PICK_CHUNK, 1000, 64.0
         c.spectrum_precision, c.template_batch, c.window_batch = SPEC_FP32, 0, 0
-        c.quirks, c.tile_size = QUIRKS_REFERENCE, 720
+        c.quirks, c.tile_size, c.cuda_graphs = QUIRKS_REFERENCE, 720, 1
         for k, v in kw.items():
             if not hasattr(c, k):
                 raise KeyError(k)
@@ -103,6 +103,10 @@ class Stats(C.Structure):
                 ("tuned_us_per_pair", C.c_double)]
 
 
+class ShardInfo(C.Structure):
+    _fields_ = [("n_pixels", C.c_size_t), ("n_windows", C.c_int), ("n_angles", C.c_int), ("pick_mode", C.c_int)]
+
+
 # Exported symbols and their ctypes signatures (kept in sync with include/gisspa.h).
 _P = C.c_void_p
 SIGNATURES = {
@@ -127,6 +131,11 @@ SIGNATURES = {
     "gisspa_cc_maps_noalloc": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.c_int, _P, _P]),
     "gisspa_debug_stage": (C.c_int, [_P, C.c_int, _P, C.c_int, C.c_int, C.POINTER(Ctf), C.c_float, _P,
                                      C.c_size_t]),
+    "gisspa_shard_begin": (C.c_int, [_P, _P, C.c_int, C.c_int, C.POINTER(Ctf), C.POINTER(ShardInfo)]),
+    "gisspa_shard_sweep": (C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
+    "gisspa_shard_export": (C.c_int, [_P, _P, _P, _P]),
+    "gisspa_shard_import": (C.c_int, [_P, _P, _P, _P]),
+    "gisspa_shard_picks": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
 }
 
 _lib = None
@@ -246,6 +255,34 @@ class Searcher:
         _check(self.h, self.lib.gisspa_refine(self.h, picks.ctypes.data, len(picks), steps,
                                               C.byref(c) if c is not None else None, params.ctypes.data))
         return picks, c, params
+
+    # ---- one micrograph across ranks (gisspa_shard_*); device pointers are ints
+    def shard_begin(self, image: np.ndarray, ctf: Ctf) -> ShardInfo:
+        image = np.ascontiguousarray(image, dtype=np.float32)
+        ny, nx = image.shape
+        info = ShardInfo()
+        _check(self.h, self.lib.gisspa_shard_begin(self.h, image.ctypes.data, nx, ny, C.byref(ctf), C.byref(info)))
+        return info
+
+    def shard_sweep(self, sweep: int, angle_begin: int, angle_end: int):
+        _check(self.h, self.lib.gisspa_shard_sweep(self.h, sweep, angle_begin, angle_end))
+
+    def shard_export(self, d_sum: int, d_sum_sq: int, d_key: int | None):
+        _check(self.h, self.lib.gisspa_shard_export(self.h, C.c_void_p(d_sum), C.c_void_p(d_sum_sq),
+                                                    C.c_void_p(d_key) if d_key else None))
+
+    def shard_import(self, d_sum: int, d_sum_sq: int, d_key: int | None):
+        _check(self.h, self.lib.gisspa_shard_import(self.h, C.c_void_p(d_sum), C.c_void_p(d_sum_sq),
+                                                    C.c_void_p(d_key) if d_key else None))
+
+    def shard_picks(self, cap: int = 1 << 20) -> np.ndarray:
+        out = np.zeros(cap, dtype=PICK_DTYPE)
+        n = C.c_size_t(0)
+        st = self.lib.gisspa_shard_picks(self.h, out.ctypes.data, cap, C.byref(n))
+        if st == ERR_CAPACITY:
+            return self.shard_picks(cap=int(n.value))
+        _check(self.h, st)
+        return out[: n.value].copy()
 
     def stats(self) -> Stats:
         s = Stats()

@@ -73,6 +73,8 @@ typedef struct gisspa_config {
   int window_batch;       /* windows per correlation pass (0 = automatic) */
   int quirks;             /* GISSPA_QUIRK_* bits */
   int tile_size;          /* norm_type=0 tile edge; reference constant 720 (utils/constants.h:5) */
+  int cuda_graphs;        /* norm_type=1 sweeps: 1 = capture one angle's launches in a CUDA graph and
+                             replay it for the other angles, 0 = launch every kernel from the host */
 } gisspa_config;
 
 /* Per-micrograph CTF, as in an LST line "defocus= dfdiff= dfang=" (DataReader2.h:93-103).
@@ -225,6 +227,44 @@ int gisspa_cc_maps(gisspa_handle* h, const void* d_windows, int n_windows, const
  * threads) race on it and must be serialised by the caller. */
 int gisspa_cc_maps_noalloc(const void* d_windows, int n_windows, const void* d_templates, int n_templates,
                            int window_size, int spec, float* d_out, void* stream);
+
+/* ---- one micrograph across several GPUs (no counterpart in the reference, whose GPUs
+ * only split the micrograph list, main.cu:51-90) ----
+ * norm_type=1 only.  Every rank holds a handle on its own GPU with the same config and
+ * templates, and takes a contiguous range of the angle sequence
+ * (for (float e = 0; e < 360; e += phistep), norm.cu:684).  The ranks' per-window-pixel
+ * state is merged by the caller's collective (sum of the two FP64 sums, max of the
+ * signed 64-bit peak keys), then:
+ *   top-K:  begin -> sweep(1, a0, a1) -> export -> [all-reduce] -> import -> picks
+ *           (every rank returns the same picks);
+ *   chunk:  begin -> sweep(1, a0, a1) -> export -> [all-reduce] -> import
+ *           -> sweep(2, a0, a1) -> picks (this rank's angles only; concatenating the
+ *           ranks' lists in angle order gives the single-GPU list).
+ * A peak key packs the largest correlation of a window pixel over this rank's
+ * template-rotations with its index k = angle * n_templates + template:
+ * ((order-preserving bits of the FP32 value) << 32 | (0xFFFFFFFF - k)) XOR 2^63, read as
+ * int64, so a signed max picks the larger value and, on ties, the lower k (as one GPU
+ * does); 0x8000000000000000 (INT64_MIN) marks a pixel with none. */
+typedef struct gisspa_shard_info {
+  size_t n_pixels;  /* window pixels W x window_size^2: length of each exported array */
+  int n_windows;    /* W */
+  int n_angles;     /* length of the angle sequence */
+  int pick_mode;    /* GISSPA_PICK_* of the handle */
+} gisspa_shard_info;
+
+/* Preparation of one micrograph (host image, as gisspa_search) and zeroed state. */
+int gisspa_shard_begin(gisspa_handle* h, const float* image, int nx, int ny, const gisspa_ctf* ctf,
+                       gisspa_shard_info* info);
+/* Sweep 1 (or 2, chunk mode, after import) over angles [angle_begin, angle_end). */
+int gisspa_shard_sweep(gisspa_handle* h, int sweep, int angle_begin, int angle_end);
+/* Copies this rank's state to caller-owned device memory on the handle's GPU, n_pixels
+ * entries each: sum and sum_sq of the correlation (FP64), and (top-K mode) the peak keys;
+ * peak_key may be NULL in chunk mode. */
+int gisspa_shard_export(gisspa_handle* h, double* sum, double* sum_sq, long long* peak_key);
+/* Loads the merged state (same layout) and computes the normalisation statistics. */
+int gisspa_shard_import(gisspa_handle* h, const double* sum, const double* sum_sq, const long long* peak_key);
+/* Picks after import (top-K) or after sweep 2 (chunk); capacity as gisspa_search. */
+int gisspa_shard_picks(gisspa_handle* h, gisspa_pick* picks, size_t cap, size_t* n_out);
 
 /* ---- diagnostics: stage outputs for parity tests (no counterpart in the reference) ---- */
 enum {
