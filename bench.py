@@ -284,7 +284,8 @@ def main():
     roofline = {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": tr,
                 "bytes_per_launch": alg, "launch_us": dur, "pass_a_us": st_a, "pass_b_us": st_b,
-                "pairs_per_launch": ppl, "templates_per_launch": dpl}
+                "pairs_per_launch": ppl, "templates_per_launch": dpl,
+                "pass_b_variant": int(stats[-1].pass_b_variant)}
 
     res = None
     if rank == 0:

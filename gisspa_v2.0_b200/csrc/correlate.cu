@@ -354,6 +354,10 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     __syncthreads();  // this stage buffer is refilled two templates later
   }
 
+  // Fold this launch's partial sums (and maxima) into the per-pixel state with reductions that
+  // return nothing, so no warp waits on the state's memory latency.  Each pixel receives one
+  // reduction per launch and launches are stream-ordered: the additions happen in the same
+  // order, with the same rounding, as a read-modify-write.
   if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll
     for (int s = 0; s < RPT; ++s) {
@@ -361,22 +365,15 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const size_t pix = wbase + (size_t)oy * L + ox[i];
-        double2* p1 = reinterpret_cast<double2*>(a.S1 + pix);
-        double2* p2 = reinterpret_cast<double2*>(a.S2 + pix);
-        double2 s1 = *p1, s2 = *p2;
-        s1.x += acc1[s][i][0];
-        s1.y += acc1[s][i][1];
-        s2.x += acc2[s][i][0];
-        s2.y += acc2[s][i][1];
-        *p1 = s1;
-        *p2 = s2;
-        if constexpr (EPI == EPI_TOPK) {
 #pragma unroll
-          for (int h = 0; h < 2; ++h)
-            if (barg[s][i][h] >= 0 && best[s][i][h] > a.cmax[pix + h]) {
-              a.cmax[pix + h] = best[s][i][h];
-              a.carg[pix + h] = barg[s][i][h];
-            }
+        for (int h = 0; h < 2; ++h) {
+          atomicAdd(a.S1 + pix + h, (double)acc1[s][i][h]);
+          atomicAdd(a.S2 + pix + h, (double)acc2[s][i][h]);
+          if constexpr (EPI == EPI_TOPK) {
+            if (barg[s][i][h] >= 0)
+              atomicMax(a.peak + pix + h, ((unsigned long long)float_key(best[s][i][h]) << 32) |
+                                              (unsigned)(0xFFFFFFFFu - (unsigned)barg[s][i][h]));
+          }
         }
       }
     }

@@ -46,8 +46,10 @@ struct CorrArgs {
   // EPI_SUM / EPI_TOPK state, [W][L][L]
   double* S1;
   double* S2;
-  float* cmax;
-  int* carg;
+  // EPI_TOPK: per pixel the best correlation and its index k = angle * nt_total + template,
+  // (float_key(c) << 32) | (0xFFFFFFFF - k), 0 = none yet: an integer max keeps the larger c
+  // and, on ties, the lower k (the first one a single sweep meets)
+  unsigned long long* peak;
   // EPI_CHUNK
   const float2* musig;      // [W][L][L] (mu, 1/sigma or 0)
   float thresh;

@@ -126,51 +126,27 @@ __global__ void musig_kernel(const double* __restrict__ S1, const double* __rest
   ms[i] = make_float2((float)mu, sd > 0 ? (float)(1.0 / sd) : 0.f);
 }
 
-__global__ void fill_kernel(float* __restrict__ a, int* __restrict__ b, long long n) {
+// Peak keys of the sharded search: the per-pixel key of the top-K sweep XOR 2^63, read as int64
+// (a signed max then orders them as the unsigned max does; 0 = none becomes INT64_MIN).
+__global__ void peak_flip_kernel(const unsigned long long* __restrict__ in, long long n,
+                                 unsigned long long* __restrict__ out) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  a[i] = -INFINITY;
-  b[i] = -1;
-}
-
-// Peak keys of the sharded search: ((float_key(c) << 32) | (0xFFFFFFFF - k)) XOR 2^63 as int64,
-// INT64_MIN for a pixel without a correlation (carg < 0).
-__global__ void peak_pack_kernel(const float* __restrict__ cmax, const int* __restrict__ carg, long long n,
-                                 long long* __restrict__ key) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int a = carg[i];
-  unsigned long long k = 0;
-  if (a >= 0) k = ((unsigned long long)float_key(cmax[i]) << 32) | (unsigned)(0xFFFFFFFFu - (unsigned)a);
-  key[i] = (long long)(k ^ 0x8000000000000000ull);
-}
-
-__global__ void peak_unpack_kernel(const long long* __restrict__ key, long long n, float* __restrict__ cmax,
-                                   int* __restrict__ carg) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const unsigned long long k = (unsigned long long)key[i] ^ 0x8000000000000000ull;
-  if (k == 0) {
-    cmax[i] = -INFINITY;
-    carg[i] = -1;
-    return;
-  }
-  cmax[i] = key_float((uint32_t)(k >> 32));
-  carg[i] = (int)(0xFFFFFFFFu - (uint32_t)(k & 0xFFFFFFFFu));
+  out[i] = in[i] ^ 0x8000000000000000ull;
 }
 
 // Top-K: image map of the max z over windows covering each pixel (ties: lowest window).
-__global__ void zmap_kernel(const float* __restrict__ cmax, const int* __restrict__ carg,
-                            const float2* __restrict__ ms, int l, const int* __restrict__ offx,
-                            const int* __restrict__ offy, int bx, int nx, int ny,
+__global__ void zmap_kernel(const unsigned long long* __restrict__ peak, const float2* __restrict__ ms, int l,
+                            const int* __restrict__ offx, const int* __restrict__ offy, int bx, int nx, int ny,
                             unsigned long long* __restrict__ zkey) {
   const int b = blockIdx.y;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= l * l) return;
   const size_t i = (size_t)b * l * l + k;
-  if (carg[i] < 0) return;
+  const unsigned long long pk = peak[i];
+  if (!pk) return;
   const float2 m = ms[i];
-  const float z = (cmax[i] - m.x) * m.y;
+  const float z = (key_float((uint32_t)(pk >> 32)) - m.x) * m.y;
   const int cx = offx[b % bx] + k % l, cy = offy[b / bx] + k / l;
   if (cx >= nx || cy >= ny) return;
   const unsigned long long key = ((unsigned long long)float_key(z) << 32) | (unsigned)(0xFFFFFFFFu - (unsigned)b);
@@ -192,7 +168,7 @@ __global__ void angle_select_kernel(const AngleState* __restrict__ table, int* _
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
 __global__ void zcompact_kernel(const unsigned long long* __restrict__ zkey, int nx, int ny, float thresh, float dmin,
-                                const int* __restrict__ carg, int l, const int* __restrict__ offx,
+                                const unsigned long long* __restrict__ peak, int l, const int* __restrict__ offx,
                                 const int* __restrict__ offy, int bx, ZCand* __restrict__ out,
                                 unsigned* __restrict__ count, unsigned cap) {
   const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -205,7 +181,8 @@ __global__ void zcompact_kernel(const unsigned long long* __restrict__ zkey, int
   const int b = (int)(0xFFFFFFFFu - (unsigned)(k & 0xFFFFFFFFu));
   const int px = x - offx[b % bx], py = y - offy[b / bx];
   const unsigned s = atomicAdd(count, 1u);
-  if (s < cap) out[s] = ZCand{z, (int)q, b, carg[(size_t)b * l * l + (size_t)py * l + px]};
+  const unsigned long long pk = peak[(size_t)b * l * l + (size_t)py * l + px];
+  if (s < cap) out[s] = ZCand{z, (int)q, b, (int)(0xFFFFFFFFu - (uint32_t)(pk & 0xFFFFFFFFu))};
 }
 
 struct Ctx {
@@ -332,15 +309,14 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
     maxE = std::max(maxE, cd.E);
     maxDE = std::max(maxDE, cd.D * cd.E);
   }
-  // scratch outputs: S1, S2 (double), cmax (float), carg (int) for maxE windows; nn arrays; counter
+  // scratch outputs: S1, S2 (double), peak keys (u64) for maxE windows; nn arrays; counter
   const size_t px = (size_t)maxE * c.L2;
   const size_t nn = (size_t)maxE * nt;
   char* base = static_cast<char*>(h->tune_scratch.ensure(px * 24 + nn * 24 + 256));
   args.S1 = reinterpret_cast<double*>(base);
   args.S2 = args.S1 + px;
-  args.cmax = reinterpret_cast<float*>(args.S2 + px);
-  args.carg = reinterpret_cast<int*>(args.cmax + px);
-  args.nn_key = reinterpret_cast<unsigned long long*>(args.carg + px);
+  args.peak = reinterpret_cast<unsigned long long*>(args.S2 + px);
+  args.nn_key = args.peak + px;
   args.nn_sum = reinterpret_cast<double*>(args.nn_key + nn);
   args.cand_count = reinterpret_cast<unsigned*>(args.nn_sum + 2 * nn);
   args.cand_cap = 0;
@@ -484,10 +460,8 @@ void norm_prepare(Ctx& c, const float* d_img, int nx, int ny, NormRun& r) {
   args.dmin = cfg.diameter;
   args.thresh = cfg.threshold;
   if (r.topk) {
-    args.cmax = buf<float>(h->cmax, r.npix);
-    args.carg = buf<int>(h->carg, r.npix);
-    fill_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, c.s>>>(args.cmax, args.carg, (long long)r.npix);
-    GISSPA_LAUNCH_CHECK();
+    args.peak = buf<unsigned long long>(h->peak, r.npix);
+    GISSPA_CUDA(cudaMemsetAsync(args.peak, 0, sizeof(unsigned long long) * r.npix, c.s));
   }
   choose_batches(cfg, l, r.W, nt, r.D, r.E);
   r.phase = 1;
@@ -512,8 +486,8 @@ std::vector<unsigned char> angle_graph_key(Ctx& c, const NormRun& r, int epi) {
   for (const void* p : {(const void*)h->prep_real.as<void>(), (const void*)h->rot.as<void>(),
                         (const void*)h->rot_tmp.as<void>(), (const void*)h->rsums.as<void>(),
                         (const void*)h->tspec.as<void>(), (const void*)h->ispec.as<void>(),
-                        (const void*)h->Q.as<void>(), (const void*)a.S1, (const void*)a.S2, (const void*)a.cmax,
-                        (const void*)a.carg, (const void*)a.musig, (const void*)a.offx, (const void*)a.offy,
+                        (const void*)h->Q.as<void>(), (const void*)a.S1, (const void*)a.S2, (const void*)a.peak,
+                        (const void*)a.musig, (const void*)a.offx, (const void*)a.offy,
                         (const void*)a.cand, (const void*)a.cand_count, (const void*)h->dev_err.as<void>(),
                         (const void*)h->angle_table.as<void>(), (const void*)h->angle_cursor.as<void>(),
                         (const void*)h->angle_cur.as<void>()})
@@ -695,7 +669,7 @@ void topk_picks(Ctx& c, NormRun& r, std::vector<gisspa_pick>& out) {
   const long long N = r.N;
   unsigned long long* zk = buf<unsigned long long>(h->zkey, N);
   GISSPA_CUDA(cudaMemsetAsync(zk, 0, sizeof(unsigned long long) * N, c.s));
-  zmap_kernel<<<dim3(ceil_div(c.L2, 256), r.W), 256, 0, c.s>>>(r.args.cmax, r.args.carg, r.args.musig, l, r.args.offx,
+  zmap_kernel<<<dim3(ceil_div(c.L2, 256), r.W), 256, 0, c.s>>>(r.args.peak, r.args.musig, l, r.args.offx,
                                                                 r.args.offy, bx, nx, ny, zk);
   GISSPA_LAUNCH_CHECK();
   unsigned cap = (unsigned)std::max<size_t>(h->zcand.size() / sizeof(ZCand), 1u << 16);
@@ -704,7 +678,7 @@ void topk_picks(Ctx& c, NormRun& r, std::vector<gisspa_pick>& out) {
     ZCand* zc = buf<ZCand>(h->zcand, cap);
     unsigned* cnt = buf<unsigned>(h->zcount, 1);
     GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
-    zcompact_kernel<<<ceil_div(N, 256), 256, 0, c.s>>>(zk, nx, ny, cfg.threshold, cfg.diameter, r.args.carg, l,
+    zcompact_kernel<<<ceil_div(N, 256), 256, 0, c.s>>>(zk, nx, ny, cfg.threshold, cfg.diameter, r.args.peak, l,
                                                         r.args.offx, r.args.offy, bx, zc, cnt, cap);
     GISSPA_LAUNCH_CHECK();
     unsigned count = 0;
@@ -1288,8 +1262,8 @@ void shard_export(gisspa_handle* h, double* sum, double* sum_sq, long long* peak
   GISSPA_CUDA(cudaMemcpyAsync(sum, r.args.S1, sizeof(double) * r.npix, cudaMemcpyDeviceToDevice, s));
   GISSPA_CUDA(cudaMemcpyAsync(sum_sq, r.args.S2, sizeof(double) * r.npix, cudaMemcpyDeviceToDevice, s));
   if (r.topk && peak_key) {
-    peak_pack_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, s>>>(r.args.cmax, r.args.carg, (long long)r.npix,
-                                                                       peak_key);
+    peak_flip_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, s>>>(
+        r.args.peak, (long long)r.npix, reinterpret_cast<unsigned long long*>(peak_key));
     GISSPA_LAUNCH_CHECK();
   }
   shard_sync(h, "shard_export");
@@ -1301,8 +1275,8 @@ void shard_import(gisspa_handle* h, const double* sum, const double* sum_sq, con
   GISSPA_CUDA(cudaMemcpyAsync(r.args.S1, sum, sizeof(double) * r.npix, cudaMemcpyDeviceToDevice, c.s));
   GISSPA_CUDA(cudaMemcpyAsync(r.args.S2, sum_sq, sizeof(double) * r.npix, cudaMemcpyDeviceToDevice, c.s));
   if (r.topk) {
-    peak_unpack_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, c.s>>>(peak_key, (long long)r.npix, r.args.cmax,
-                                                                           r.args.carg);
+    peak_flip_kernel<<<ceil_div((long long)r.npix, 256), 256, 0, c.s>>>(
+        reinterpret_cast<const unsigned long long*>(peak_key), (long long)r.npix, r.args.peak);
     GISSPA_LAUNCH_CHECK();
   }
   norm_stats(c, r);

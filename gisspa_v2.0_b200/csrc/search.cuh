@@ -75,7 +75,7 @@ struct gisspa_handle {
   // shells, statistics
   gisspa::DevBuf ra, rb, stats, scratch;
   // per-window-pixel state
-  gisspa::DevBuf S1, S2, cmax, carg, musig;
+  gisspa::DevBuf S1, S2, peak, musig;
   // correlation intermediate and outputs
   gisspa::DevBuf Q, cand, cand_count, nn_key, nn_sum, zkey, zcand, zcount;
   gisspa::DevBuf dev_err;  // set by kernels whose bounded waits gave up
