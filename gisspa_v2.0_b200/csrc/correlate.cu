@@ -6,20 +6,19 @@
 namespace gisspa {
 namespace {
 
-struct BlockSync {
-  __device__ __forceinline__ void operator()() const { __syncthreads(); }
-};
 struct WarpSync {
   __device__ __forceinline__ void operator()() const { __syncwarp(); }
 };
 
 template <int L>
 struct PassA;
-template <> struct PassA<256> { static constexpr int TT = 32, NC = 16; };
-template <> struct PassA<512> { static constexpr int TT = 64, NC = 8; };
-template <> struct PassA<1024> { static constexpr int TT = 64, NC = 4; };
+template <> struct PassA<256> { static constexpr int TT = 16, NC = 16; };
+template <> struct PassA<512> { static constexpr int TT = 16, NC = 16; };
+template <> struct PassA<1024> { static constexpr int TT = 32, NC = 8; };
 
 // Pass A: one team of TT threads per column slot, NC slots per CTA, one pair per blockIdx.y.
+// Each column is a two-stage Stockham transform (32 x 16 points at L = 512) with E = L / TT
+// points per thread: one exchange through the team's slice of shared memory, inside a warp.
 // The column transforms leave row-major, Q[pair][y][slot], through a shared tile: each team
 // writes its column with the slot XOR-swizzled by the row (slot ^ (y mod NC)), and rows are
 // read back as 16-byte pairs, so both sides are free of bank conflicts and every row segment
@@ -27,13 +26,14 @@ template <> struct PassA<1024> { static constexpr int TT = 64, NC = 4; };
 // 2^SH rows per 128-byte line, so 16 consecutive rows of one column fall in 16 distinct bank
 // pairs.
 template <int L, typename SPEC>
-__global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
+__global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC, 2)
     pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
                   int b0, int n0, int D, const float2* __restrict__ twL) {
   constexpr int TT = PassA<L>::TT, NC = PassA<L>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
   constexpr int SH = NC >= 16 ? 0 : NC == 8 ? 1 : 2;
   static_assert(NC == 4 || NC == 8 || NC == 16, "swizzle assumes 4, 8 or 16 slots per CTA");
-  __shared__ __align__(16) float2 smem[NC * L];  // FFT exchange buffers, then the output tile
+  static_assert(TT <= 32 && 32 % TT == 0, "a team lies inside one warp");
+  extern __shared__ __align__(16) float2 smem[];  // [NC * L]: FFT exchange buffers, then the output tile
   const int team = threadIdx.x / TT, tid = threadIdx.x - team * TT;
   const int c0 = blockIdx.x * NC, c = c0 + team;
   const int p = blockIdx.y;
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
     // columns kx = 0 and kx = L/2 have real inverse transforms: pack them as a + i b
 #pragma unroll
     for (int i = 0; i < E; ++i) {
-      const int ky = fft3_in_index<L, TT>(tid, i);
+      const int ky = fft2_in_index<L, TT>(tid, i);
       const float2 a = cmulc(Ib[ky], SPEC::load(Tn + ky));
       const float2 b = cmulc(Ib[(size_t)NZ * L + ky], SPEC::load(Tn + (size_t)NZ * L + ky));
       v[i] = make_float2(a.x - b.y, a.y + b.x);
@@ -55,15 +55,15 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC)
     const typename SPEC::T* Tc = Tn + (size_t)c * L;
 #pragma unroll
     for (int i = 0; i < E; ++i) {
-      const int ky = fft3_in_index<L, TT>(tid, i);
+      const int ky = fft2_in_index<L, TT>(tid, i);
       v[i] = cmulc(__ldg(Ic + ky), SPEC::load(Tc + ky));
     }
   }
-  fft3<L, TT, +1>(v, smem + team * L, TwGlobal{twL}, tid, BlockSync{});
+  fft2s<L, TT, +1>(v, smem + team * L, TwGlobal{twL}, tid, WarpSync{});
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < E; ++i) {
-    const int y = fft3_out_index<L, TT>(tid, i);
+    const int y = fft2_out_index<L, TT>(tid, i);
     smem[y * NC + (team ^ ((y >> SH) & (NC - 1)))] = v[i];
   }
   __syncthreads();
@@ -384,8 +384,14 @@ template <int L, typename SPEC>
 void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
               const float2* twL, cudaStream_t s) {
   constexpr int NZ = L / 2;
+  constexpr size_t smem = (size_t)PassA<L>::NC * L * sizeof(float2);
+  static bool configured = false;
+  if (!configured) {
+    GISSPA_CUDA(cudaFuncSetAttribute(pass_a_kernel<L, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
   dim3 grid(NZ / PassA<L>::NC, cl.E * cl.D);
-  pass_a_kernel<L, SPEC><<<grid, PassA<L>::TT * PassA<L>::NC, 0, s>>>(
+  pass_a_kernel<L, SPEC><<<grid, PassA<L>::TT * PassA<L>::NC, smem, s>>>(
       I, static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL);
   GISSPA_LAUNCH_CHECK();
 }

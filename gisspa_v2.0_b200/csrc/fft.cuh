@@ -22,7 +22,23 @@ namespace gisspa {
 template <int S>
 __host__ __device__ constexpr int fft_swz(int i) { return (i & ~15) | ((i ^ (i >> S)) & 15); }
 
-// Multiply v by W_R^K = exp(SIGN * 2 pi i K / R) with exact special cases.
+// cos(2 pi k / 32) and sin(2 pi k / 32) for any integer k, from cos(j pi / 16), j = 0..8.
+__host__ __device__ constexpr double cos32(int k) {
+  constexpr double c[9] = {1.0,
+                           0.98078528040323044913,
+                           0.92387953251128675613,
+                           0.83146961230254523708,
+                           0.70710678118654752440,
+                           0.55557023301960222474,
+                           0.38268343236508977173,
+                           0.19509032201612826785,
+                           0.0};
+  k &= 31;
+  return k <= 8 ? c[k] : k <= 16 ? -c[16 - k] : k <= 24 ? -c[k - 16] : c[32 - k];
+}
+__host__ __device__ constexpr double sin32(int k) { return cos32(k - 8); }
+
+// Multiply v by W_R^K = exp(SIGN * 2 pi i K / R) (R dividing 32) with exact special cases.
 template <int R, int K, int SIGN>
 __device__ __forceinline__ float2 mul_wr(float2 v) {
   constexpr int KK = K % R;
@@ -41,12 +57,9 @@ __device__ __forceinline__ float2 mul_wr(float2 v) {
     constexpr float h = 0.70710678118654752440f;
     return make_float2(h * (-v.x - SIGN * v.y), h * (-v.y + SIGN * v.x));
   } else {
-    // R == 16, odd K: angles k * pi / 8
-    constexpr double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;
-    constexpr int k8 = (16 / R) * KK;  // in units of 2 pi / 16
-    constexpr double cc = (k8 == 1) ? c1 : (k8 == 3) ? s1 : (k8 == 5) ? -s1 : -c1;
-    constexpr double ss = (k8 == 1) ? s1 : (k8 == 3) ? c1 : (k8 == 5) ? c1 : s1;
-    constexpr float c = (float)cc, s = (float)(SIGN * ss);
+    static_assert(32 % R == 0, "radix must divide 32");
+    constexpr int k32 = (32 / R) * KK;  // in units of 2 pi / 32
+    constexpr float c = (float)cos32(k32), s = (float)(SIGN * sin32(k32));
     return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
   }
 }
@@ -108,7 +121,7 @@ __device__ __forceinline__ float2 table_tw(const Tw& tw, int p) {
 // is log2(R) products from w1, so each power carries a few ulp beyond the table entry.
 template <int M, int R>
 struct TwPow {
-  static constexpr int H = M >= 8 ? 8 : M >= 4 ? 4 : M >= 2 ? 2 : 1;  // highest power of two <= M
+  static constexpr int H = M >= 16 ? 16 : M >= 8 ? 8 : M >= 4 ? 4 : M >= 2 ? 2 : 1;  // highest power of 2 <= M
   __device__ __forceinline__ static void run(float2* w) {
     if constexpr (M < R) {
       w[M] = (H == M) ? cmul(w[M / 2], w[M / 2]) : cmul(w[H], w[M - H]);
@@ -118,7 +131,7 @@ struct TwPow {
 };
 template <int R>
 __device__ __forceinline__ void tw_powers(float2 w1, float2* w) {
-  static_assert(R <= 16, "powers up to 15");
+  static_assert(R <= 32, "powers up to 31");
   w[1] = w1;
   TwPow<2, R>::run(w);
 }
@@ -208,6 +221,37 @@ __device__ __forceinline__ int fft3_in_index(int tid, int e) {
   constexpr int R1 = Plan<N, T>::R1;
   const int q = e / R1, m = e % R1;
   return tid + T * q + m * (N / R1);
+}
+
+// Two-stage plans (radix R1 then R2, R1 * R2 = N) for teams of T <= 32 threads, E = N / T
+// points per thread: one shared-memory exchange, one twiddle stage, and a team inside one warp
+// (the exchange needs only __syncwarp).
+template <int N, int T>
+struct Plan2;
+template <> struct Plan2<256, 16> { static constexpr int R1 = 16, R2 = 16, S = 4; };
+template <> struct Plan2<512, 16> { static constexpr int R1 = 32, R2 = 16, S = 5; };
+template <> struct Plan2<1024, 32> { static constexpr int R1 = 32, R2 = 32, S = 5; };
+
+template <int N, int T, int SIGN, typename Sync, typename Tw>
+__device__ __forceinline__ void fft2s(float2* v, float2* sm, const Tw& tw, int tid, Sync sync) {
+  using P = Plan2<N, T>;
+  static_assert(P::R1 * P::R2 == N, "plan must factor N");
+  stockham_stage<N, T, P::R1, 1, SIGN, false, P::S>(v, sm, tw, tid);
+  sync();
+  stockham_load<N, T, P::R2, P::S>(v, sm, tid);
+  stockham_stage<N, T, P::R2, P::R1, SIGN, true, P::S>(v, sm, tw, tid);
+}
+// Index of input element e held by thread tid before fft2s.
+template <int N, int T>
+__device__ __forceinline__ int fft2_in_index(int tid, int e) {
+  constexpr int R1 = Plan2<N, T>::R1;
+  return tid + T * (e / R1) + (e % R1) * (N / R1);
+}
+// Index of output element e held by thread tid after fft2s.
+template <int N, int T>
+__device__ __forceinline__ int fft2_out_index(int tid, int e) {
+  constexpr int R2 = Plan2<N, T>::R2;
+  return tid + T * (e / R2) + (e % R2) * (N / R2);
 }
 
 }  // namespace gisspa
