@@ -414,10 +414,17 @@ void launch_b_cfg(const CorrLaunch& cl, const CorrArgs& args, const float2* twL,
 // Pass B shapes (rows per CTA RB, warps NW, min CTAs per SM) per window size and variant.
 template <int L, int V>
 struct PassB;
+// A launch has L x E row chains (a window row over the launch's D templates).  Large CTAs
+// share the bulk copies and tables; CTAs of one or two rows spread the chains evenly over the
+// SMs when L x E is not much larger than the warps the GPU holds (e.g. 2048 chains at E = 4).
 template <> struct PassB<256, 0> { static constexpr int TEAM = 16, RB = 16, NW = 8, MINB = 2; };
+template <> struct PassB<256, 1> { static constexpr int TEAM = 16, RB = 4, NW = 2, MINB = 8; };
 template <> struct PassB<512, 0> { static constexpr int TEAM = 32, RB = 16, NW = 16, MINB = 1; };
 template <> struct PassB<512, 1> { static constexpr int TEAM = 32, RB = 8, NW = 8, MINB = 2; };
+template <> struct PassB<512, 2> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 8; };
+template <> struct PassB<512, 3> { static constexpr int TEAM = 32, RB = 1, NW = 1, MINB = 16; };
 template <> struct PassB<1024, 0> { static constexpr int TEAM = 32, RB = 8, NW = 8, MINB = 1; };
+template <> struct PassB<1024, 1> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 2; };
 
 template <int L, int V>
 void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ, cudaStream_t s) {
@@ -444,12 +451,17 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
   }
   if (ev) GISSPA_CUDA(cudaEventRecord(ev[1], s));
   if constexpr (L == 512) {
+    switch (cl.variant) {
+      case 1: launch_b<L, 1>(cl, args, twL, twNZ, s); break;
+      case 2: launch_b<L, 2>(cl, args, twL, twNZ, s); break;
+      case 3: launch_b<L, 3>(cl, args, twL, twNZ, s); break;
+      default: launch_b<L, 0>(cl, args, twL, twNZ, s); break;
+    }
+  } else {
     if (cl.variant == 1)
       launch_b<L, 1>(cl, args, twL, twNZ, s);
     else
       launch_b<L, 0>(cl, args, twL, twNZ, s);
-  } else {
-    launch_b<L, 0>(cl, args, twL, twNZ, s);
   }
   if (ev) GISSPA_CUDA(cudaEventRecord(ev[2], s));
   return 2;
@@ -459,7 +471,7 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
 
 bool correlate_supported(int L) { return L == 256 || L == 512 || L == 1024; }
 
-int correlate_variants(int L) { return L == 512 ? 2 : 1; }
+int correlate_variants(int L) { return L == 512 ? 4 : 2; }
 
 int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {
