@@ -52,6 +52,8 @@ def args_parse():
     ap.add_argument("--form", default="plain", choices=list(FORMS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--chosen", default="fp16_topk", choices=list(FORMS) + ["none"],
+                    help="with --form plain: also time this form on the same micrograph (reported as chosen_form)")
     return ap.parse_args()
 
 
@@ -287,6 +289,34 @@ def main():
                 "pairs_per_launch": ppl, "templates_per_launch": dpl,
                 "pass_b_variant": int(stats[-1].pass_b_variant)}
 
+    # the chosen form on the same micrograph: FP16 spectra, one top-K sweep (the numerator of
+    # the target ratio against the plain FP32 two-sweep form timed above)
+    chosen = None
+    if a.form == "plain" and a.chosen not in ("none", "plain"):
+        p2 = dict(synth.SEARCH_PARAMS[wl])
+        p2.update(FORMS[a.chosen])
+        s2 = gisspa.Searcher(gisspa.Config.default(**p2), local)
+        s2.set_templates(case.templates)
+        for _ in range(a.warmup):
+            s2.search_device(d_img.data_ptr(), nx, ny, ctf, out)
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(a.steps):
+            n2 = s2.search_device(d_img.data_ptr(), nx, ny, ctf, out)
+        ev1.record()
+        torch.cuda.synchronize()
+        barrier()
+        t2 = torch.tensor([ev0.elapsed_time(ev1)], device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
+        v2 = world * a.steps / (float(t2.item()) / 1000.0)
+        st2 = s2.stats()
+        chosen = {"form": a.chosen, "value": v2, "unit": "micrographs/s", "ms_per_step": float(t2.item()) / a.steps,
+                  "vs_plain": v2 / value, "picks_per_step": int(n2), "pass_a_us": st2.pass_a_us,
+                  "pass_b_us": st2.pass_b_us}
+        s2.close()
+
     res = None
     if rank == 0:
         res = {"metric": METRIC, "value": value, "unit": "micrographs/s", "n_gpus": world, "steps": a.steps,
@@ -299,6 +329,8 @@ def main():
                "stage_ms": {"prep": stats[-1].ms_prep, "sweep1": stats[-1].ms_sweep1,
                             "sweep2": stats[-1].ms_sweep2, "pick": stats[-1].ms_pick},
                "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "e2e": e2e}
+        if chosen is not None:
+            res["chosen_form"] = chosen
         if world == 1 and not a.no_cpu_baseline:
             rate, cores, secs, per_rot, prep = oracle_rate(case, cfg, angles)
             res["cpu_baseline"] = {"value": rate, "unit": "micrographs/s", "cores": cores, "kind": "port",

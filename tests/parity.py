@@ -32,6 +32,11 @@ SMALL = {
                           defocus=1.8, dfdiff=0.1, dfang=30.0),
                      dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                           diameter=100.0, threshold=3.0, window_size=512, overlap=0, norm_type=1)),
+    # l = 1024 windows (the 8192^2 workload's window size) on a 1536^2 micrograph, 2x2 windows
+    "norm_l1024_w4": (dict(shape=(1536, 1536), n_particles=6, snr=0.5, n_templates=3, tsize=160, seed=24,
+                           defocus=1.7, dfdiff=0.1, dfang=30.0),
+                      dict(angpix=1.0, phistep=90.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                           diameter=120.0, threshold=3.0, window_size=1024, overlap=512, norm_type=1)),
     # norm_type=0 on 720^2 tiles of a 1024^2 micrograph with 512 windows (the tiled workload's geometry)
     "nonorm_l512": (dict(shape=(1024, 1024), n_particles=10, snr=0.5, n_templates=4, tsize=128, seed=23,
                          defocus=1.5, dfdiff=0.0, dfang=0.0),

@@ -99,7 +99,7 @@ def run_both(name, **over):
     return g, o, cfg, s
 
 
-@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4"])
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4", "norm_l1024_w4"])
 def test_search_norm_chunk_picks(name):
     g, o, cfg, s = run_both(name)
     rep = compare_chunk_picks(g, o, cfg.threshold)
@@ -122,9 +122,9 @@ def test_search_norm_stats_maps():
     assert rel_err(sd_g, sd_o) < 1e-4
 
 
-def test_search_norm_topk():
-    g, o, cfg, s = run_both("norm_l256_w9", pick_mode=gisspa.PICK_TOPK, topk=20, exclusion_radius=30.0,
-                            threshold=2.0)
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l1024_w4"])
+def test_search_norm_topk(name):
+    g, o, cfg, s = run_both(name, pick_mode=gisspa.PICK_TOPK, topk=20, exclusion_radius=30.0, threshold=2.0)
     assert len(o) > 0 and len(g) == len(o)
     n_same = sum(1 for a, b in zip(g, o) if (a["x"], a["y"], a["template_id"], a["angle_index"]) ==
                  (b["x"], b["y"], b["template_id"], b["angle_index"]))
