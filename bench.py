@@ -52,6 +52,8 @@ def args_parse():
     ap.add_argument("--form", default="plain", choices=list(FORMS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch", default=None,
+                    help="D,E: fix templates x windows per correlation launch instead of autotuning (profiling)")
     ap.add_argument("--chosen", default="fp16_topk", choices=list(FORMS) + ["none"],
                     help="with --form plain: also time this form on the same micrograph (reported as chosen_form)")
     return ap.parse_args()
@@ -131,14 +133,19 @@ def algorithmic_bytes(L: int, spec: int, D: float):
     return pass_a, pass_b
 
 
-def traffic_from_profiles(kernel: str):
-    """DRAM bytes per launch from the committed ncu summary, when present."""
+def traffic_from_profiles(kernel: str, spec: int, pairs_per_launch: float):
+    """DRAM bytes per launch: the per-pair dram__bytes_read.sum + dram__bytes_write.sum of the
+    committed ncu capture (profiles/ncu_traffic.json, warm caches, the bench workload with a
+    fixed launch shape) times this run's pairs per launch; None when absent."""
     p = os.path.join(REPO, "profiles", "ncu_traffic.json")
     try:
         with open(p) as fh:
-            return json.load(fh).get(kernel)
+            t = json.load(fh)
     except Exception:
         return None
+    key = f"{kernel}/{'fp32' if spec == gisspa.SPEC_FP32 else 'fp16'}"
+    e = t.get(key) or t.get(kernel)
+    return None if e is None else float(e["bytes_per_pair"]) * pairs_per_launch
 
 
 # ------------------------------------------------------------------ CPU leg (the FP64 oracle)
@@ -171,6 +178,8 @@ def main():
     wl = a.workload
     params = dict(synth.SEARCH_PARAMS[wl])
     params.update(FORMS[a.form])
+    if a.batch:
+        params["template_batch"], params["window_batch"] = (int(x) for x in a.batch.split(","))
     cfg = gisspa.Config.default(**params)
     angles = int(math.ceil(360.0 / cfg.phistep - 1e-9))
     data = dict(synth.WORKLOADS[wl])
@@ -282,7 +291,7 @@ def main():
     dur = st_b if kern == "pass_b" else st_a
     alg = (bb if kern == "pass_b" else ba) * ppl
     achieved = alg / (dur * 1e-6) / 1e9 if dur > 0 else 0.0
-    tr = traffic_from_profiles(kern)
+    tr = traffic_from_profiles(kern, cfg.spectrum_precision, ppl)
     roofline = {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": tr,
                 "bytes_per_launch": alg, "launch_us": dur, "pass_a_us": st_a, "pass_b_us": st_b,
