@@ -52,6 +52,8 @@ def args_parse():
     ap.add_argument("--form", default="plain", choices=list(FORMS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch every kernel from the host (cuda_graphs = 0), e.g. for per-launch profiling")
     ap.add_argument("--batch", default=None,
                     help="D,E: fix templates x windows per correlation launch instead of autotuning (profiling)")
     ap.add_argument("--chosen", default="fp16_topk", choices=list(FORMS) + ["none"],
@@ -180,6 +182,8 @@ def main():
     params.update(FORMS[a.form])
     if a.batch:
         params["template_batch"], params["window_batch"] = (int(x) for x in a.batch.split(","))
+    if a.eager:
+        params["cuda_graphs"] = 0
     cfg = gisspa.Config.default(**params)
     angles = int(math.ceil(360.0 / cfg.phistep - 1e-9))
     data = dict(synth.WORKLOADS[wl])
