@@ -425,6 +425,8 @@ template <> struct PassB<512, 2> { static constexpr int TEAM = 32, RB = 2, NW = 
 template <> struct PassB<512, 3> { static constexpr int TEAM = 32, RB = 1, NW = 1, MINB = 16; };
 template <> struct PassB<1024, 0> { static constexpr int TEAM = 32, RB = 8, NW = 8, MINB = 1; };
 template <> struct PassB<1024, 1> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 2; };
+// the same, capped at 168 registers (6 CTAs per SM): no spills for the sum and chunk epilogues
+template <> struct PassB<1024, 2> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 6; };
 
 template <int L, int V>
 void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ, cudaStream_t s) {
@@ -457,6 +459,12 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
       case 3: launch_b<L, 3>(cl, args, twL, twNZ, s); break;
       default: launch_b<L, 0>(cl, args, twL, twNZ, s); break;
     }
+  } else if constexpr (L == 1024) {
+    switch (cl.variant) {
+      case 1: launch_b<L, 1>(cl, args, twL, twNZ, s); break;
+      case 2: launch_b<L, 2>(cl, args, twL, twNZ, s); break;
+      default: launch_b<L, 0>(cl, args, twL, twNZ, s); break;
+    }
   } else {
     if (cl.variant == 1)
       launch_b<L, 1>(cl, args, twL, twNZ, s);
@@ -471,7 +479,7 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
 
 bool correlate_supported(int L) { return L == 256 || L == 512 || L == 1024; }
 
-int correlate_variants(int L) { return L == 512 ? 4 : 2; }
+int correlate_variants(int L) { return L == 512 ? 4 : L == 1024 ? 3 : 2; }
 
 int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {
