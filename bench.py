@@ -48,7 +48,9 @@ def args_parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="whole_4096_t200", choices=list(synth.WORKLOADS))
+    ap.add_argument("--workload", default="whole_4096_t200", choices=list(synth.WORKLOADS) + ["batch_c3"])
+    ap.add_argument("--batch-n", type=int, default=8,
+                    help="batch_c3: micrographs per gisspa_search_batch call (the first n of the 32-micrograph batch)")
     ap.add_argument("--form", default="plain", choices=list(FORMS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -171,6 +173,71 @@ def oracle_rate(case, cfg, n_angles: int):
     return 1.0 / mic_s, oracle.num_threads(), sum(t), per_rot, prep
 
 
+# ------------------------------------------------------------------ batching workload
+def bench_batch(a, rank: int, world: int, local: int):
+    """One step = one gisspa_search_batch call over n uneven micrographs (2048^2, 3710x3838,
+    4096^2, 4092x5760 in turn, each with its own CTF) from host memory, 500 templates of 200^2,
+    120 angles: the batching form (uneven sizes, per-micrograph CTF, graph-replayed angles)."""
+    import torch
+
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cases = [synth.make_case(**c) for c in synth.batch_cases(n=a.batch_n, seed=3 + 100 * rank)]
+    forms = [a.form] + ([a.chosen] if a.form == "plain" and a.chosen not in ("none", "plain") else [])
+    res_forms = {}
+    for form in forms:
+        params = dict(synth.SEARCH_PARAMS["batch_c3"])
+        params.update(FORMS[form])
+        cfg = gisspa.Config.default(**params)
+        s = gisspa.Searcher(cfg, local)
+        s.set_templates(cases[0].templates)
+        imgs = [c.image for c in cases]
+        ctfs = [gisspa.Ctf(c.defocus, c.dfdiff, c.dfang) for c in cases]
+        for _ in range(a.warmup):
+            s.search_batch(imgs, ctfs)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(a.steps):
+            picks = s.search_batch(imgs, ctfs)
+        ev1.record()
+        torch.cuda.synchronize()
+        t = torch.tensor([ev0.elapsed_time(ev1)], device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        st = s.stats()
+        n_rot = cases[0].templates.shape[0] * int(math.ceil(360.0 / cfg.phistep - 1e-9))
+        res_forms[form] = {"value": world * a.steps * len(cases) / (ms / 1000.0), "ms_per_step": ms / a.steps,
+                           "template_rotations_per_s": world * a.steps * len(cases) * n_rot / (ms / 1000.0),
+                           "pairs_per_step": int(st.pairs), "picks_per_step": int(sum(len(p) for p in picks)),
+                           "gpu_launches": int(st.kernel_launches)}
+        s.close()
+    if rank == 0:
+        main_form = res_forms[a.form]
+        res = {"metric": METRIC, "value": main_form["value"], "unit": "micrographs/s", "n_gpus": world,
+               "steps": a.steps, "warmup": a.warmup, "ms_per_step": main_form["ms_per_step"],
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded Gaussian-blob projections planted in N(0,1) noise)",
+               "config": {"workload": "batch_c3", "form": a.form, "micrographs_per_step": len(cases),
+                          "sizes": [list(c.image.shape) for c in cases], "templates": 500, "template_size": 200,
+                          "angles": 120, "window_size": 512, "overlap": 200, "norm_type": 1,
+                          "parallelism": f"replicas{world}", "entry": "gisspa_search_batch (host images)"},
+               "forms": res_forms}
+        if len(forms) > 1:
+            res["chosen_form"] = {"form": forms[1], **res_forms[forms[1]],
+                                  "vs_plain": res_forms[forms[1]]["value"] / main_form["value"]}
+        print(json.dumps(res))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 # ------------------------------------------------------------------ main
 def main():
     a = args_parse()
@@ -178,6 +245,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     wl = a.workload
+    if wl == "batch_c3":
+        if a.impl == "reference":
+            raise SystemExit("the reference arm runs the single-micrograph workloads")
+        return bench_batch(a, rank, world, local)
     params = dict(synth.SEARCH_PARAMS[wl])
     params.update(FORMS[a.form])
     if a.batch:

@@ -161,6 +161,9 @@ SEARCH_PARAMS = {
                             diameter=140.0, threshold=7.0, window_size=512, overlap=192, norm_type=1),
     "whole_8192_t1000": dict(angpix=1.0, phistep=5.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                              diameter=200.0, threshold=7.0, window_size=1024, overlap=256, norm_type=1),
+    # batching: uneven micrographs (batch_cases), 500 templates of 200^2, 3 degree step
+    "batch_c3": dict(angpix=1.0, phistep=3.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                     diameter=150.0, threshold=7.0, window_size=512, overlap=200, norm_type=1),
     "whole_2048_t24": dict(angpix=1.0, phistep=90.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                            diameter=140.0, threshold=7.0, window_size=512, overlap=192, norm_type=1),
 }
