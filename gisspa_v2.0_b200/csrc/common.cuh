@@ -63,6 +63,13 @@ struct AngleState {
   int pad;
 };
 
+// Programmatic dependent launch (sm_90+): a kernel launched with programmatic stream
+// serialization may start before its predecessor finishes; griddep_wait blocks until the
+// predecessor has completed and its memory is visible (a no-op for a normal launch), and
+// griddep_launch_dependents lets the successor start as soon as every CTA has issued it.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 // Order-preserving map of a float onto uint32 (larger float -> larger key).
 __device__ __forceinline__ uint32_t float_key(float f) {
   uint32_t b = __float_as_uint(f);

@@ -1,4 +1,6 @@
 // correlate.cu — pass A (multiply + column IFFT) and pass B (row C2R + epilogue).
+#include <utility>
+
 #include "../../include/gisspa.h"
 #include "correlate.cuh"
 #include "fft.cuh"
@@ -28,7 +30,7 @@ template <> struct PassA<1024> { static constexpr int TT = 32, NC = 8; };
 template <int L, typename SPEC>
 __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC, 2)
     pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
-                  int b0, int n0, int D, const float2* __restrict__ twL) {
+                  int b0, int n0, int D, const float2* __restrict__ twL, int chained) {
   constexpr int TT = PassA<L>::TT, NC = PassA<L>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
   constexpr int SH = NC >= 16 ? 0 : NC == 8 ? 1 : 2;
   static_assert(NC == 4 || NC == 8 || NC == 16, "swizzle assumes 4, 8 or 16 slots per CTA");
@@ -38,6 +40,8 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC, 2)
   const int c0 = blockIdx.x * NC, c = c0 + team;
   const int p = blockIdx.y;
   const int e = p / D, d = p - e * D;
+  griddep_launch_dependents();
+  if (!chained) griddep_wait();  // the spectra may come from the kernel just before
   const float2* Ib = I + (size_t)(b0 + e) * HS * L;
   const typename SPEC::T* Tn = T + (size_t)(n0 + d) * HS * L;
   float2 v[E];
@@ -67,6 +71,7 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC, 2)
     smem[y * NC + (team ^ ((y >> SH) & (NC - 1)))] = v[i];
   }
   __syncthreads();
+  if (chained) griddep_wait();  // Q is still being read by the previous pass B
   float2* Qp = Q + (size_t)p * L * NZ + c0;
   constexpr int HALF = NC / 2;  // 16-byte pairs per row segment
   for (int u = threadIdx.x; u < L * HALF; u += TT * NC) {
@@ -135,6 +140,8 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     fence_mbar_init();
   }
   __syncthreads();
+  griddep_launch_dependents();
+  griddep_wait();  // Q comes from the pass A just before
   auto issue = [&](int d) {
     const float2* src = a.Q + ((size_t)(e * a.D + d) * L + y0) * NZ;
     fence_proxy_async_smem();
@@ -380,6 +387,24 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   }
 }
 
+// Launch with programmatic stream serialization (the kernel's griddep_wait orders it after
+// its predecessor).
+template <typename... P, typename... A>
+void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  GISSPA_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+  ++launch_counter();
+}
+
 template <int L, typename SPEC>
 void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
               const float2* twL, cudaStream_t s) {
@@ -391,9 +416,8 @@ void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, c
     configured = true;
   }
   dim3 grid(NZ / PassA<L>::NC, cl.E * cl.D);
-  pass_a_kernel<L, SPEC><<<grid, PassA<L>::TT * PassA<L>::NC, smem, s>>>(
-      I, static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL);
-  GISSPA_LAUNCH_CHECK();
+  launch_pdl(pass_a_kernel<L, SPEC>, grid, dim3(PassA<L>::TT * PassA<L>::NC), smem, s, I,
+             static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0);
 }
 
 template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
@@ -407,8 +431,7 @@ void launch_b_cfg(const CorrLaunch& cl, const CorrArgs& args, const float2* twL,
     configured = true;
   }
   dim3 grid(L / RB, cl.E);
-  pass_b_kernel<L, TEAM, RB, NW, EPI, MINB><<<grid, NW * 32, smem, s>>>(args, twL, twNZ);
-  GISSPA_LAUNCH_CHECK();
+  launch_pdl(pass_b_kernel<L, TEAM, RB, NW, EPI, MINB>, grid, dim3(NW * 32), smem, s, args, twL, twNZ);
 }
 
 // Pass B shapes (rows per CTA RB, warps NW, min CTAs per SM) per window size and variant.

@@ -75,6 +75,10 @@ struct CorrLaunch {
   int spec;           // GISSPA_SPEC_*
   int epi;            // Epilogue
   int variant = 0;    // pass B shape (see correlate_variants)
+  // Pass A directly follows the previous launch's pass B on the stream and reads nothing that
+  // pass B writes: it then waits for it only before storing Q (programmatic dependent launch
+  // overlaps the rest with pass B's last CTAs).  Otherwise pass A waits at its start.
+  bool chained = false;
 };
 
 // Launch pass A then pass B on stream s.  I: window spectra [W][L/2+1][L];

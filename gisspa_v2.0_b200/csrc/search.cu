@@ -375,6 +375,7 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
     for (int b0 = 0; b0 < W; b0 += E) {
       const int e = std::min(E, W - b0);
       CorrLaunch cl{l, e, d, h->cfg.spectrum_precision, epi, variant};
+      cl.chained = pairs > 0;  // after this sequence's first pair of passes
       args.Q = Q;
       args.b0 = b0;
       args.n0 = n0;
