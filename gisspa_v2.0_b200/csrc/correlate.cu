@@ -1,4 +1,5 @@
 // correlate.cu — pass A (multiply + column IFFT) and pass B (row C2R + epilogue).
+#include <mutex>
 #include <utility>
 
 #include "../../include/gisspa.h"
@@ -10,6 +11,18 @@ namespace {
 
 struct WarpSync {
   __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+// Barrier of one team of TEAM > 32 threads (whole warps): named barrier `id` (1..15; 0 is
+// __syncthreads) counting TEAM threads.
+template <int TEAM>
+struct TeamSync {
+  int id;
+  __device__ __forceinline__ void operator()() const {
+    if constexpr (TEAM <= 32)
+      __syncwarp();
+    else
+      asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(TEAM) : "memory");
+  }
 };
 
 template <int L>
@@ -117,7 +130,8 @@ __device__ __forceinline__ bool team_any(bool pred) {
 template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB)
     pass_b_kernel(CorrArgs a, const float2* __restrict__ twL, const float2* __restrict__ twNZ) {
-  constexpr int NZ = L / 2, E = NZ / TEAM, TPW = 32 / TEAM, NTEAM = NW * TPW, RPT = RB / NTEAM;
+  constexpr int NZ = L / 2, E = NZ / TEAM, NTEAM = NW * 32 / TEAM, RPT = RB / NTEAM;
+  static_assert(TEAM <= 32 || (TEAM % 32 == 0 && NTEAM <= 15), "a wide team is whole warps with its own barrier");
   constexpr unsigned kStageBytes = RB * NZ * sizeof(float2);
   static_assert(RB % NTEAM == 0, "rows must split evenly over teams");
   extern __shared__ __align__(128) float2 stage[];  // [2][RB][NZ]
@@ -231,8 +245,9 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         const float2 o = cmul(w, od);
         v[i] = make_float2(ev.x - o.y, ev.y + o.x);
       }
-      __syncwarp();
-      fft3<NZ, TEAM, +1>(v, row, TwShared{tw_nz}, lt, WarpSync{});
+      const TeamSync<TEAM> tsync{1 + team};
+      tsync();  // every lane of the team has read the row before the transform overwrites it
+      fft3<NZ, TEAM, +1>(v, row, TwShared{tw_nz}, lt, tsync);
 
       if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll
@@ -250,6 +265,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
             }
           }
       } else if constexpr (EPI == EPI_CHUNK) {
+        static_assert(TEAM <= 32, "chunk maxima reduce within a warp");
         float z[E][2];
         float zmax = -INFINITY;
 #pragma unroll
@@ -306,6 +322,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
           }
         }
       } else if constexpr (EPI == EPI_NONORM) {
+        static_assert(TEAM <= 32, "peak and sums reduce within a warp");
         constexpr int CPR = L >= 256 ? L / 256 : 1;
         // get_peak_and_SUM (kernels.cu:725-763): sums over every pixel, max with the
         // border (closer than diameter/4 to the window edge) forced to 0
@@ -387,6 +404,23 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   }
 }
 
+// Runs f once per device for one kernel instance (cudaFuncSetAttribute acts on the current
+// device only, and one process may drive several GPUs from several threads).
+struct PerDeviceOnce {
+  std::mutex m;
+  unsigned long long done = 0;  // bit per device ordinal
+  template <typename F>
+  void operator()(F&& f) {
+    int dev = 0;
+    GISSPA_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(m);
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done & bit)) return;
+    f();
+    done |= bit;
+  }
+};
+
 // Launch with programmatic stream serialization (the kernel's griddep_wait orders it after
 // its predecessor).
 template <typename... P, typename... A>
@@ -410,11 +444,10 @@ void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, c
               const float2* twL, cudaStream_t s) {
   constexpr int NZ = L / 2;
   constexpr size_t smem = (size_t)PassA<L>::NC * L * sizeof(float2);
-  static bool configured = false;
-  if (!configured) {
+  static PerDeviceOnce once;
+  once([] {
     GISSPA_CUDA(cudaFuncSetAttribute(pass_a_kernel<L, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+  });
   dim3 grid(NZ / PassA<L>::NC, cl.E * cl.D);
   launch_pdl(pass_a_kernel<L, SPEC>, grid, dim3(PassA<L>::TT * PassA<L>::NC), smem, s, I,
              static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0);
@@ -424,12 +457,11 @@ template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
 void launch_b_cfg(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ,
                   cudaStream_t s) {
   constexpr size_t smem = 2 * (size_t)RB * (L / 2) * sizeof(float2);
-  static bool configured = false;
-  if (!configured) {
+  static PerDeviceOnce once;
+  once([] {
     GISSPA_CUDA(cudaFuncSetAttribute(pass_b_kernel<L, TEAM, RB, NW, EPI, MINB>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+  });
   dim3 grid(L / RB, cl.E);
   launch_pdl(pass_b_kernel<L, TEAM, RB, NW, EPI, MINB>, grid, dim3(NW * 32), smem, s, args, twL, twNZ);
 }
@@ -450,10 +482,22 @@ template <> struct PassB<1024, 0> { static constexpr int TEAM = 32, RB = 8, NW =
 template <> struct PassB<1024, 1> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 2; };
 // the same, capped at 168 registers (6 CTAs per SM): no spills for the sum and chunk epilogues
 template <> struct PassB<1024, 2> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 6; };
+// 64-lane rows (8 points and 16 pixels per lane: half the accumulators), sum / top-K / map only
+template <> struct PassB<1024, 3> { static constexpr int TEAM = 64, RB = 2, NW = 4, MINB = 4; };
+template <> struct PassB<1024, 4> { static constexpr int TEAM = 64, RB = 1, NW = 2, MINB = 8; };
 
 template <int L, int V>
 void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ, cudaStream_t s) {
   using P = PassB<L, V>;
+  if constexpr (P::TEAM > 32) {
+    switch (cl.epi) {
+      case EPI_SUM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_SUM, P::MINB>(cl, args, twL, twNZ, s); break;
+      case EPI_TOPK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_TOPK, P::MINB>(cl, args, twL, twNZ, s); break;
+      case EPI_MAP: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_MAP, P::MINB>(cl, args, twL, twNZ, s); break;
+      default: throw CudaError{cudaErrorInvalidValue, "pass B shape without this epilogue"};
+    }
+    return;
+  } else {
   switch (cl.epi) {
     case EPI_SUM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_SUM, P::MINB>(cl, args, twL, twNZ, s); break;
     case EPI_CHUNK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_CHUNK, P::MINB>(cl, args, twL, twNZ, s); break;
@@ -461,6 +505,7 @@ void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, con
     case EPI_NONORM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_NONORM, P::MINB>(cl, args, twL, twNZ, s); break;
     case EPI_MAP: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_MAP, P::MINB>(cl, args, twL, twNZ, s); break;
     default: throw CudaError{cudaErrorInvalidValue, "unknown epilogue"};
+  }
   }
 }
 
@@ -486,6 +531,8 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
     switch (cl.variant) {
       case 1: launch_b<L, 1>(cl, args, twL, twNZ, s); break;
       case 2: launch_b<L, 2>(cl, args, twL, twNZ, s); break;
+      case 3: launch_b<L, 3>(cl, args, twL, twNZ, s); break;
+      case 4: launch_b<L, 4>(cl, args, twL, twNZ, s); break;
       default: launch_b<L, 0>(cl, args, twL, twNZ, s); break;
     }
   } else {
@@ -502,7 +549,13 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
 
 bool correlate_supported(int L) { return L == 256 || L == 512 || L == 1024; }
 
-int correlate_variants(int L) { return L == 512 ? 4 : L == 1024 ? 3 : 2; }
+int correlate_variants(int L) { return L == 512 ? 4 : L == 1024 ? 5 : 2; }
+
+bool correlate_variant_ok(int L, int variant, int epi) {
+  if (variant < 0 || variant >= correlate_variants(L)) return false;
+  const bool wide = L == 1024 && variant >= 3;  // 64-lane rows
+  return !wide || epi == EPI_SUM || epi == EPI_TOPK || epi == EPI_MAP;
+}
 
 int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {

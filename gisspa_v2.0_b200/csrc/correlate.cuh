@@ -92,5 +92,7 @@ int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float
 bool correlate_supported(int L);
 // Number of pass B shapes compiled for a window size (the autotuner's choices).
 int correlate_variants(int L);
+// Whether pass B shape `variant` has epilogue `epi`.
+bool correlate_variant_ok(int L, int variant, int epi);
 
 }  // namespace gisspa

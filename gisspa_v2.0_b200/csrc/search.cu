@@ -331,6 +331,7 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   best.us_per_pair = 1e30;
   for (int v = 0; v < correlate_variants(l); ++v)
     for (const auto& cd : cands) {
+      if (!correlate_variant_ok(l, v, epi)) continue;
       CorrLaunch cl{l, cd.E, cd.D, h->cfg.spectrum_precision, epi, v};
       args.b0 = 0;
       args.n0 = 0;
