@@ -395,4 +395,16 @@ int gisspa_format_pick(const gisspa_pick* p, int lst_index, const char* path, co
   return n;
 }
 
+int gisspa_debug_wait_probe(gisspa_handle* h, double seconds) {
+  if (!h) return GISSPA_ERR_ARG;
+  if (!(seconds > 0.0) || seconds > 10.0) {
+    h->err = "wait_probe: seconds must lie in (0, 10]";
+    return GISSPA_ERR_ARG;
+  }
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    wait_probe(h, seconds);
+  });
+}
+
 }  // extern "C"

@@ -167,6 +167,20 @@ __global__ void angle_select_kernel(const AngleState* __restrict__ table, int* _
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
+// A bounded wait on an mbarrier phase that never completes (its single expected arrival is
+// never made, and no asynchronous copy targets it): the wait gives up after max_cycles and the
+// CTA raises the error flag, exactly as pass B does when its bulk copies do not land.
+__global__ void wait_probe_kernel(unsigned* err, long long max_cycles) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const bool ok = mbar_wait(&bar, 0, max_cycles);
+  if (!__syncthreads_and(ok) && threadIdx.x == 0) atomicOr(err, 1u);
+}
+
 __global__ void zcompact_kernel(const unsigned long long* __restrict__ zkey, int nx, int ny, float thresh, float dmin,
                                 const unsigned long long* __restrict__ peak, int l, const int* __restrict__ offx,
                                 const int* __restrict__ offy, int bx, ZCand* __restrict__ out,
@@ -1158,6 +1172,19 @@ void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int n
   unsigned flag = 0;
   GISSPA_CUDA(cudaMemcpy(&flag, args.err, sizeof(flag), cudaMemcpyDeviceToHost));
   if (flag) throw TimeoutError{"cc_maps"};
+}
+
+void wait_probe(gisspa_handle* h, double seconds) {
+  int khz = 0;
+  GISSPA_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, h->device));
+  unsigned* err = buf<unsigned>(h->dev_err, 1);
+  GISSPA_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), h->stream));
+  wait_probe_kernel<<<1, 32, 0, h->stream>>>(err, (long long)(seconds * 1e3 * (double)std::max(khz, 1)));
+  GISSPA_LAUNCH_CHECK();
+  GISSPA_CUDA(cudaStreamSynchronize(h->stream));
+  unsigned flag = 0;
+  GISSPA_CUDA(cudaMemcpy(&flag, err, sizeof(flag), cudaMemcpyDeviceToHost));
+  if (flag) throw TimeoutError{"the wait probe"};
 }
 
 void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const gisspa_ctf& ctf,

@@ -157,6 +157,8 @@ void shard_sweep(gisspa_handle* h, int sweep, int a0, int a1);
 void shard_export(gisspa_handle* h, double* sum, double* sum_sq, long long* peak_key);
 void shard_import(gisspa_handle* h, const double* sum, const double* sum_sq, const long long* peak_key);
 void shard_picks(gisspa_handle* h, std::vector<gisspa_pick>& out);
+// Bounded device wait that is made to run out (gisspa_debug_wait_probe); throws TimeoutError.
+void wait_probe(gisspa_handle* h, double seconds);
 int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx, const int* ny,
               const gisspa_ctf* ctfs, gisspa_pick* picks, size_t cap, size_t* offsets);
 

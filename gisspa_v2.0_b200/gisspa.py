@@ -136,6 +136,7 @@ SIGNATURES = {
     "gisspa_shard_export": (C.c_int, [_P, _P, _P, _P]),
     "gisspa_shard_import": (C.c_int, [_P, _P, _P, _P]),
     "gisspa_shard_picks": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "gisspa_debug_wait_probe": (C.c_int, [_P, C.c_double]),
 }
 
 _lib = None

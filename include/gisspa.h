@@ -280,6 +280,13 @@ enum {
 int gisspa_debug_stage(gisspa_handle* h, int what, const float* image, int nx, int ny, const gisspa_ctf* ctf,
                        float theta, void* out, size_t bytes);
 
+/* Failure-path check (no counterpart in the reference, which has no device waits): one
+ * kernel waits, through the same bounded mbarrier wait the correlation kernels use, for an
+ * arrival that never comes, gives up after `seconds` (0 < seconds <= 10) and raises the
+ * handle's device error flag.  Returns GISSPA_ERR_TIMEOUT, as a search whose bulk copies
+ * never landed would; the handle stays usable. */
+int gisspa_debug_wait_probe(gisspa_handle* h, double seconds);
+
 #ifdef __cplusplus
 }
 #endif

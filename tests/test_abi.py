@@ -89,3 +89,12 @@ def test_null_handle_is_an_argument_error():
     n = C.c_size_t(0)
     assert lib.gisspa_search(None, None, 0, 0, None, None, 0, C.byref(n)) == gisspa.ERR_ARG
     assert lib.gisspa_set_templates(None, None, 0, 0, 0) == gisspa.ERR_ARG
+
+
+def test_null_handle_new_entry_points():
+    lib = gisspa.load()
+    n = C.c_size_t(0)
+    assert lib.gisspa_shard_sweep(None, 1, 0, 1) == gisspa.ERR_ARG
+    assert lib.gisspa_shard_export(None, None, None, None) == gisspa.ERR_ARG
+    assert lib.gisspa_shard_picks(None, None, 0, C.byref(n)) == gisspa.ERR_ARG
+    assert lib.gisspa_debug_wait_probe(None, 0.1) == gisspa.ERR_ARG
