@@ -171,3 +171,25 @@ def test_batch_matches_single_searches():
     both = s.search_batch([img, img2], [ctf, ctf])
     for x, y in zip(one, both):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4"])
+def test_chosen_form_picks_and_scores(name):
+    """The chosen form (FP16 template spectra, one top-K sweep) against the FP64 oracle: every
+    pick whose score stands clear of the other picks' by more than the tolerance is found at
+    the same (x, y, template, angle), and peak scores agree within 1e-3 (relative)."""
+    tol = 1e-3
+    g, o, cfg, s = run_both(name, spectrum_precision=gisspa.SPEC_FP16, pick_mode=gisspa.PICK_TOPK, topk=30,
+                            exclusion_radius=30.0, threshold=2.5)
+    assert len(o) >= 5
+    key = lambda p: (float(p["x"]), float(p["y"]), int(p["template_id"]), int(p["angle_index"]))
+    G = {key(p): float(p["score"]) for p in g}
+    sc = np.sort(o["score"].astype(np.float64))
+    for p in o:
+        z = float(p["score"])
+        others = sc[np.abs(sc - z) > 0] if np.sum(sc == z) == 1 else sc
+        clear = np.min(np.abs(others - z)) > 2 * tol * abs(z) if len(others) else True
+        if clear:
+            assert key(p) in G, (key(p), z)
+        if key(p) in G:
+            assert abs(G[key(p)] - z) <= tol * abs(z), (key(p), G[key(p)], z)
