@@ -265,7 +265,14 @@ __global__ void __launch_bounds__(NW * 32, MINB)
             }
           }
       } else if constexpr (EPI == EPI_CHUNK) {
-        static_assert(TEAM <= 32, "chunk maxima reduce within a warp");
+        constexpr int CPR = L >= 256 ? L / 256 : 1;  // chunks per row
+        // a team wider than a warp (two warps per row) meets in shared memory: the warps'
+        // votes and chunk maxima, behind the team's barrier (the next writes come after the
+        // next row's barriers)
+        constexpr int WT = TEAM > 32 ? TEAM / 32 : 1;
+        __shared__ int chunk_vote[TEAM > 32 ? NTEAM : 1][WT];
+        __shared__ unsigned long long chunk_key[TEAM > 32 ? NTEAM : 1][WT][CPR];
+        const int wid = TEAM > 32 ? (lt >> 5) : 0;
         float z[E][2];
         float zmax = -INFINITY;
 #pragma unroll
@@ -276,10 +283,18 @@ __global__ void __launch_bounds__(NW * 32, MINB)
             z[i][h] = (c - ms[s][i][h].x) * ms[s][i][h].y;
             zmax = fmaxf(zmax, z[i][h]);
           }
-        // warp-uniform branch: the shuffles below use the full warp mask, so both
-        // half-warp teams (TEAM = 16) must enter together
-        if (__any_sync(0xffffffffu, zmax >= a.thresh)) {
-          constexpr int CPR = L >= 256 ? L / 256 : 1;  // chunks per row
+        // warp-uniform (and, for wide teams, team-uniform) branch: the shuffles below use the
+        // full warp mask, so both half-warp teams (TEAM = 16) must enter together
+        bool hit = __any_sync(0xffffffffu, zmax >= a.thresh);
+        if constexpr (TEAM > 32) {
+          if ((threadIdx.x & 31) == 0) chunk_vote[team][wid] = hit;
+          tsync();
+          hit = false;
+#pragma unroll
+          for (int w = 0; w < WT; ++w) hit = hit || chunk_vote[team][w];
+        }
+        if (hit) {
+          unsigned long long keys[CPR];
 #pragma unroll
           for (int ch = 0; ch < CPR; ++ch) {
             unsigned long long key = 0;
@@ -294,7 +309,22 @@ __global__ void __launch_bounds__(NW * 32, MINB)
                     ((unsigned long long)float_key(z[i][h]) << 32) | (unsigned)(255 - brev8(t));
                 key = k2 > key ? k2 : key;
               }
-            key = team_max_u64<TEAM>(key);
+            keys[ch] = team_max_u64<(TEAM > 32 ? 32 : TEAM)>(key);
+          }
+          if constexpr (TEAM > 32) {
+            if ((threadIdx.x & 31) == 0)
+#pragma unroll
+              for (int ch = 0; ch < CPR; ++ch) chunk_key[team][wid][ch] = keys[ch];
+            tsync();
+            if (lt == 0)
+#pragma unroll
+              for (int ch = 0; ch < CPR; ++ch)
+#pragma unroll
+                for (int w = 1; w < WT; ++w) keys[ch] = keys[ch] > chunk_key[team][w][ch] ? keys[ch] : chunk_key[team][w][ch];
+          }
+#pragma unroll
+          for (int ch = 0; ch < CPR; ++ch) {
+            const unsigned long long key = keys[ch];
             if (lt == 0) {
               const float zb = key_float((uint32_t)(key >> 32));
               if (zb >= a.thresh) {
@@ -482,7 +512,8 @@ template <> struct PassB<1024, 0> { static constexpr int TEAM = 32, RB = 8, NW =
 template <> struct PassB<1024, 1> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 2; };
 // the same, capped at 168 registers (6 CTAs per SM): no spills for the sum and chunk epilogues
 template <> struct PassB<1024, 2> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 6; };
-// 64-lane rows (8 points and 16 pixels per lane: half the accumulators), sum / top-K / map only
+// 64-lane rows (8 points and 16 pixels per lane: half the accumulators); every epilogue but
+// norm_type=0's
 template <> struct PassB<1024, 3> { static constexpr int TEAM = 64, RB = 2, NW = 4, MINB = 4; };
 template <> struct PassB<1024, 4> { static constexpr int TEAM = 64, RB = 1, NW = 2, MINB = 8; };
 
@@ -493,6 +524,7 @@ void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, con
     switch (cl.epi) {
       case EPI_SUM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_SUM, P::MINB>(cl, args, twL, twNZ, s); break;
       case EPI_TOPK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_TOPK, P::MINB>(cl, args, twL, twNZ, s); break;
+      case EPI_CHUNK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_CHUNK, P::MINB>(cl, args, twL, twNZ, s); break;
       case EPI_MAP: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_MAP, P::MINB>(cl, args, twL, twNZ, s); break;
       default: throw CudaError{cudaErrorInvalidValue, "pass B shape without this epilogue"};
     }
@@ -554,7 +586,7 @@ int correlate_variants(int L) { return L == 512 ? 4 : L == 1024 ? 5 : 2; }
 bool correlate_variant_ok(int L, int variant, int epi) {
   if (variant < 0 || variant >= correlate_variants(L)) return false;
   const bool wide = L == 1024 && variant >= 3;  // 64-lane rows
-  return !wide || epi == EPI_SUM || epi == EPI_TOPK || epi == EPI_MAP;
+  return !wide || epi == EPI_SUM || epi == EPI_TOPK || epi == EPI_CHUNK || epi == EPI_MAP;
 }
 
 int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,

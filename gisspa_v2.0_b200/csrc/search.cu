@@ -87,6 +87,20 @@ int validate_config(const gisspa_config& c, std::string& err) {
     err = "template_batch and window_batch must be >= 0";
     return GISSPA_ERR_ARG;
   }
+  if (c.pass_b_shape < -1 || c.pass_b_shape >= correlate_variants(l)) {
+    err = "pass_b_shape must be -1 or one of the " + std::to_string(correlate_variants(l)) +
+          " shapes compiled for window_size " + std::to_string(l);
+    return GISSPA_ERR_ARG;
+  }
+  if (c.pass_b_shape >= 0) {
+    const int epis[3] = {c.norm_type == 0 ? EPI_NONORM : (c.pick_mode == GISSPA_PICK_TOPK ? EPI_TOPK : EPI_SUM),
+                         c.norm_type == 0 ? EPI_NONORM : EPI_CHUNK, EPI_MAP};
+    for (int k = 0; k < (c.norm_type != 0 && c.pick_mode == GISSPA_PICK_CHUNK ? 2 : 1); ++k)
+      if (!correlate_variant_ok(l, c.pass_b_shape, epis[k])) {
+        err = "pass_b_shape " + std::to_string(c.pass_b_shape) + " has no epilogue for this search";
+        return GISSPA_ERR_UNSUPPORTED;
+      }
+  }
   return GISSPA_OK;
 }
 
@@ -369,6 +383,11 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
   gisspa_handle* h = c.h;
   const int l = c.l;
   int variant = 0;
+  if (h->cfg.template_batch > 0 && h->cfg.window_batch > 0 && h->cfg.pass_b_shape >= 0) {
+    if (!correlate_variant_ok(l, h->cfg.pass_b_shape, epi))
+      throw CudaError{cudaErrorInvalidValue, "pass_b_shape not compiled for this window size and epilogue"};
+    variant = h->cfg.pass_b_shape;
+  }
   if (h->cfg.template_batch == 0 && h->cfg.window_batch == 0) {
     const long long key = (long long)l | ((long long)epi << 16) | ((long long)h->cfg.spectrum_precision << 24) |
                           ((long long)std::min(nt, 64) << 32) | ((long long)std::min(W, 64) << 40);

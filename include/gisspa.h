@@ -75,6 +75,8 @@ typedef struct gisspa_config {
   int tile_size;          /* norm_type=0 tile edge; reference constant 720 (utils/constants.h:5) */
   int cuda_graphs;        /* norm_type=1 sweeps: 1 = capture one angle's launches in a CUDA graph and
                              replay it for the other angles, 0 = launch every kernel from the host */
+  int pass_b_shape;       /* with template_batch and window_batch set: row-transform kernel shape
+                             (0.. compiled shapes - 1; -1 = the first); ignored when autotuning */
 } gisspa_config;
 
 /* Per-micrograph CTF, as in an LST line "defocus= dfdiff= dfang=" (DataReader2.h:93-103).

@@ -193,3 +193,30 @@ def test_chosen_form_picks_and_scores(name):
             assert key(p) in G, (key(p), z)
         if key(p) in G:
             assert abs(G[key(p)] - z) <= tol * abs(z), (key(p), G[key(p)], z)
+
+
+@pytest.mark.parametrize("name,shapes", [("norm_l256_w9", 2), ("norm_l512_w4", 4), ("norm_l1024_w4", 5)])
+@pytest.mark.parametrize("mode", ["chunk", "topk"])
+def test_every_row_kernel_shape(name, shapes, mode):
+    """Each compiled row-transform shape (forced with fixed launch batches) against the oracle."""
+    img, tmpl, ctf, cfg = small_case(name)
+    over = dict(template_batch=2, window_batch=2)
+    if mode == "topk":
+        over.update(pick_mode=gisspa.PICK_TOPK, topk=20, exclusion_radius=30.0, threshold=2.0)
+    cfg = cfg.copy(**over)
+    o = oracle.search(cfg, ctf, img, tmpl)
+    assert len(o) > 0
+    for v in range(shapes):
+        s = gisspa.Searcher(cfg.copy(pass_b_shape=v))
+        s.set_templates(tmpl)
+        g = s.search(img, ctf)
+        if mode == "chunk":
+            rep = compare_chunk_picks(g, o, cfg.threshold)
+            assert rep["missing"] == 0 and rep["extra"] == 0 and rep["score_bad"] == 0, (v, rep)
+            assert rep["pos_bad"] <= max(1, len(o) // 200), (v, rep)
+        else:
+            assert len(g) == len(o), v
+            same = sum(1 for a, b in zip(g, o) if (a["x"], a["y"], a["template_id"], a["angle_index"]) ==
+                       (b["x"], b["y"], b["template_id"], b["angle_index"]))
+            assert same >= len(o) - 1, v
+            assert np.allclose(np.sort(g["score"]), np.sort(o["score"]), rtol=SCORE_RTOL, atol=SCORE_ATOL), v
