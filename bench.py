@@ -48,7 +48,8 @@ def args_parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="whole_4096_t200", choices=list(synth.WORKLOADS) + ["batch_c3"])
+    ap.add_argument("--workload", default="whole_4096_t200",
+                    choices=list(synth.WORKLOADS) + ["batch_c3", "project_c5"])
     ap.add_argument("--batch-n", type=int, default=8,
                     help="batch_c3: micrographs per gisspa_search_batch call (the first n of the 32-micrograph batch)")
     ap.add_argument("--form", default="plain", choices=list(FORMS))
@@ -238,6 +239,51 @@ def bench_batch(a, rank: int, world: int, local: int):
         torch.distributed.destroy_process_group()
 
 
+# ------------------------------------------------------------------ template generation workload
+def bench_project(a, rank: int, local: int):
+    """One step = the 1000 projections of 256^2 that the 8192^2 workload searches, made from a
+    256^3 map (seeded Gaussian blobs) through gisspa_project: host volume in, host stack out."""
+    import torch
+
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(9 + rank)
+    size, n = 256, 1000
+    zz, yy, xx = np.mgrid[0:size, 0:size, 0:size].astype(np.float32)
+    vol = np.zeros((size, size, size), np.float32)
+    for c, sg in zip(rng.uniform(0.3 * size, 0.7 * size, (40, 3)), rng.uniform(3.0, 8.0, 40)):
+        vol += np.exp(-((xx - c[0]) ** 2 + (yy - c[1]) ** 2 + (zz - c[2]) ** 2) / (2 * sg * sg)).astype(np.float32)
+    angles = rng.uniform(0.0, 2 * np.pi, (n, 3)).astype(np.float32)
+    params = dict(synth.SEARCH_PARAMS["whole_8192_t1000"])
+    s = gisspa.Searcher(gisspa.Config.default(**params), local)
+    for _ in range(a.warmup):
+        s.project(vol, angles)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        s.project(vol, angles)
+    el = time.perf_counter() - t0
+    value = a.steps * n / el
+    res = {"metric": "projections/s (template generation, emdata::project3d semantics)", "value": value,
+           "unit": "projections/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": 1000.0 * el / a.steps, "higher_is_better": True, "dtype": "f32 (f64 z-interpolation)",
+           "data": "synthetic 256^3 Gaussian-blob map, uniform random Euler angles",
+           "config": {"workload": "project_c5", "volume": [size] * 3, "projections": n,
+                      "timing": "host wall clock around gisspa_project (volume H2D, projections D2H inside)"}}
+    if not a.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle
+
+        k = 16
+        t0 = time.perf_counter()
+        oracle.project3d(vol, angles[:k])
+        cpu = k / (time.perf_counter() - t0)
+        res["cpu_baseline"] = {"value": cpu, "unit": "projections/s", "cores": oracle.num_threads(), "kind": "port",
+                               "sample": f"oracle restatement (bit-identical to the reference's project3d), {k} projections"}
+    s.close()
+    if rank == 0:
+        print(json.dumps(res))
+
+
 # ------------------------------------------------------------------ main
 def main():
     a = args_parse()
@@ -249,6 +295,10 @@ def main():
         if a.impl == "reference":
             raise SystemExit("the reference arm runs the single-micrograph workloads")
         return bench_batch(a, rank, world, local)
+    if wl == "project_c5":
+        if a.impl == "reference":
+            raise SystemExit("the reference arm runs the single-micrograph workloads")
+        return bench_project(a, rank, local)
     params = dict(synth.SEARCH_PARAMS[wl])
     params.update(FORMS[a.form])
     if a.batch:

@@ -396,6 +396,60 @@ int gisspa_format_pick(const gisspa_pick* p, int lst_index, const char* path, co
   return n;
 }
 
+namespace {
+int check_projection(gisspa_handle* h, const char* what, const float* volume, int nx, int ny, int nz,
+                     const float* angles, int n, int ri) {
+  if (!volume || !angles || n <= 0 || nx < 2 || ny < 2 || nz < 2 || ri < 0) {
+    h->err = std::string(what) + ": need a volume of at least 2^3, n > 0 angles and ri >= 0";
+    return GISSPA_ERR_ARG;
+  }
+  if ((long long)nx * ny * nz > (1LL << 31) || (long long)n * nx * ny > (1LL << 31)) {
+    h->err = std::string(what) + ": volume or projection stack above 2^31 floats";
+    return GISSPA_ERR_SHAPE;
+  }
+  return GISSPA_OK;
+}
+}  // namespace
+
+int gisspa_project(gisspa_handle* h, const float* volume, int nx, int ny, int nz, const float* angles, int n,
+                   int ri, float* out) {
+  if (!h) return GISSPA_ERR_ARG;
+  int st = check_projection(h, "project", volume, nx, ny, nz, angles, n, ri);
+  if (st) return st;
+  if (!out) {
+    h->err = "project: null output";
+    return GISSPA_ERR_ARG;
+  }
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    const size_t np = (size_t)n * nx * ny;
+    float* d = static_cast<float*>(h->proj_out.ensure(sizeof(float) * np));
+    project_run(h, volume, nx, ny, nz, angles, n, ri, d);
+    GISSPA_CUDA(cudaMemcpy(out, d, sizeof(float) * np, cudaMemcpyDeviceToHost));
+  });
+}
+
+int gisspa_set_templates_from_volume(gisspa_handle* h, const float* volume, int nx, int ny, int nz,
+                                     const float* angles, int n, int ri) {
+  if (!h) return GISSPA_ERR_ARG;
+  int st = check_projection(h, "set_templates_from_volume", volume, nx, ny, nz, angles, n, ri);
+  if (st) return st;
+  if (nx > h->cfg.window_size || ny > h->cfg.window_size) {
+    h->err = "set_templates_from_volume: projection " + std::to_string(nx) + "x" + std::to_string(ny) +
+             " larger than window_size " + std::to_string(h->cfg.window_size);
+    return GISSPA_ERR_SHAPE;
+  }
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    float* d = static_cast<float*>(h->d_stack.ensure(sizeof(float) * (size_t)n * nx * ny));
+    project_run(h, volume, nx, ny, nz, angles, n, ri, d);
+    h->nt = n;
+    h->tw = nx;
+    h->th = ny;
+    h->templates_ready = true;
+  });
+}
+
 int gisspa_debug_wait_probe(gisspa_handle* h, double seconds) {
   if (!h) return GISSPA_ERR_ARG;
   if (!(seconds > 0.0) || seconds > 10.0) {

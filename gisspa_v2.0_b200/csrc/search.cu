@@ -10,6 +10,7 @@
 #include "adjoint.cuh"
 #include "correlate.cuh"
 #include "prep.cuh"
+#include "project.cuh"
 #include "search.cuh"
 
 namespace gisspa {
@@ -1191,6 +1192,19 @@ void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int n
   unsigned flag = 0;
   GISSPA_CUDA(cudaMemcpy(&flag, args.err, sizeof(flag), cudaMemcpyDeviceToHost));
   if (flag) throw TimeoutError{"cc_maps"};
+}
+
+void project_run(gisspa_handle* h, const float* volume, int nx, int ny, int nz, const float* angles, int n, int ri,
+                 float* d_out) {
+  const size_t nv = (size_t)nx * ny * nz;
+  float* dv = buf<float>(h->proj_vol, nv);
+  GISSPA_CUDA(cudaMemcpyAsync(dv, volume, sizeof(float) * nv, cudaMemcpyHostToDevice, h->stream));
+  std::vector<float> mx;
+  projection_matrices(angles, n, mx);
+  float* dm = buf<float>(h->proj_mx, mx.size());
+  GISSPA_CUDA(cudaMemcpyAsync(dm, mx.data(), sizeof(float) * mx.size(), cudaMemcpyHostToDevice, h->stream));
+  project_volume(dv, projection_geometry(nx, ny, nz, ri), dm, n, d_out, h->stream);
+  GISSPA_CUDA(cudaStreamSynchronize(h->stream));
 }
 
 void wait_probe(gisspa_handle* h, double seconds) {

@@ -88,6 +88,7 @@ struct gisspa_handle {
   std::vector<int> last_offx, last_offy;
   std::vector<float> last_angles;
   gisspa::NormRun run;  // the norm_type=1 search in progress (sharded entry points)
+  gisspa::DevBuf proj_vol, proj_mx, proj_out;  // template generation
   // CUDA-graph replay of the sweeps' angles
   std::vector<gisspa::AngleGraph> graphs;
   gisspa::DevBuf angle_table, angle_cursor, angle_cur;
@@ -157,6 +158,9 @@ void shard_sweep(gisspa_handle* h, int sweep, int a0, int a1);
 void shard_export(gisspa_handle* h, double* sum, double* sum_sq, long long* peak_key);
 void shard_import(gisspa_handle* h, const double* sum, const double* sum_sq, const long long* peak_key);
 void shard_picks(gisspa_handle* h, std::vector<gisspa_pick>& out);
+// Projections of a host volume at host angles into device memory d_out (n x ny x nx).
+void project_run(gisspa_handle* h, const float* volume, int nx, int ny, int nz, const float* angles, int n, int ri,
+                 float* d_out);
 // Bounded device wait that is made to run out (gisspa_debug_wait_probe); throws TimeoutError.
 void wait_probe(gisspa_handle* h, double seconds);
 int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx, const int* ny,

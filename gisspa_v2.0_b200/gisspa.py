@@ -137,6 +137,8 @@ SIGNATURES = {
     "gisspa_shard_import": (C.c_int, [_P, _P, _P, _P]),
     "gisspa_shard_picks": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "gisspa_debug_wait_probe": (C.c_int, [_P, C.c_double]),
+    "gisspa_project": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, C.c_int, _P]),
+    "gisspa_set_templates_from_volume": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, C.c_int]),
 }
 
 _lib = None
@@ -256,6 +258,23 @@ class Searcher:
         _check(self.h, self.lib.gisspa_refine(self.h, picks.ctypes.data, len(picks), steps,
                                               C.byref(c) if c is not None else None, params.ctypes.data))
         return picks, c, params
+
+    # ---- template generation (projections of a 3D map, emdata::project3d semantics)
+    def project(self, volume: np.ndarray, angles, ri: int = 0) -> np.ndarray:
+        vol = np.ascontiguousarray(volume, dtype=np.float32)
+        nz, ny, nx = vol.shape
+        ang = np.ascontiguousarray(np.asarray(angles, dtype=np.float32).reshape(-1, 3))
+        out = np.zeros((len(ang), ny, nx), dtype=np.float32)
+        _check(self.h, self.lib.gisspa_project(self.h, vol.ctypes.data, nx, ny, nz, ang.ctypes.data, len(ang), ri,
+                                               out.ctypes.data))
+        return out
+
+    def set_templates_from_volume(self, volume: np.ndarray, angles, ri: int = 0):
+        vol = np.ascontiguousarray(volume, dtype=np.float32)
+        nz, ny, nx = vol.shape
+        ang = np.ascontiguousarray(np.asarray(angles, dtype=np.float32).reshape(-1, 3))
+        _check(self.h, self.lib.gisspa_set_templates_from_volume(self.h, vol.ctypes.data, nx, ny, nz,
+                                                                 ang.ctypes.data, len(ang), ri))
 
     # ---- one micrograph across ranks (gisspa_shard_*); device pointers are ints
     def shard_begin(self, image: np.ndarray, ctf: Ctf) -> ShardInfo:

@@ -230,6 +230,21 @@ int gisspa_cc_maps(gisspa_handle* h, const void* d_windows, int n_windows, const
 int gisspa_cc_maps_noalloc(const void* d_windows, int n_windows, const void* d_templates, int n_templates,
                            int window_size, int spec, float* d_out, void* stream);
 
+/* ---- template generation on the device ----
+ * The reference searches a template stack made beforehand, by projecting a 3D map with EMAN's
+ * project3d (EMReader/emdata.cpp:891-996).  These calls make that stack on the GPU, bit for
+ * bit as project3d does with zero translation (its dx, dy members, which no constructor or
+ * reader of the reference sets) and the volume's own depth.  The volume is [nz][ny][nx] floats
+ * in host memory, angles are n (alt, az, phi) triples in radians (project3d's units), ri is
+ * the mask radius in pixels (0: nx/2). */
+/* Projections into host memory out: n x ny x nx floats. */
+int gisspa_project(gisspa_handle* h, const float* volume, int nx, int ny, int nz, const float* angles, int n,
+                   int ri, float* out);
+/* The projections become this handle's template stack (as gisspa_set_templates, without the
+ * host round trip). */
+int gisspa_set_templates_from_volume(gisspa_handle* h, const float* volume, int nx, int ny, int nz,
+                                     const float* angles, int n, int ri);
+
 /* ---- one micrograph across several GPUs (no counterpart in the reference, whose GPUs
  * only split the micrograph list, main.cu:51-90) ----
  * norm_type=1 only.  Every rank holds a handle on its own GPU with the same config and

@@ -914,4 +914,64 @@ int orc_search_nonorm(const gisspa_config* cin, const gisspa_ctf* ctf, const flo
 
 int orc_num_threads(void) { return omp_get_max_threads(); }
 
+// Projection of a volume [nz][ny][nx] along Euler angles (alt, az, phi; radians) as the
+// reference's emdata::project3d (EMReader/emdata.cpp:891-996) computes it, with its
+// translation (dx, dy) zero and its depth the volume's (the members it reads; see the
+// projection harness oracle/ref_project_main.cpp):
+//  * the rotation matrix in double from C's double cos/sin, stored as float (emdata.cpp:913-921);
+//  * mask radius rmax = ri (nx/2 when ri <= 0), sphere r^2 >= i^2 + j^2 + k^2 in float, i and j
+//    over [-rmax + 0.5, rmax + 0.5) truncated and clamped to [-n/2, n/2] (emdata.cpp:934-939);
+//  * the in-plane source coordinates are truncated to int (x2, y2 are int at emdata.cpp:899),
+//    so of the trilinear weights only the one along z survives: (1 - v) p(z) + v p(z + 1)
+//    in double (emdata.h:173-179), added in float to the output pixel, k ascending.
+int orc_project3d(const float* vol, int nx, int ny, int nz, const float* angles, int n, int ri, float* out) {
+  if (nx <= 0 || ny <= 0 || nz <= 0 || n < 0) return GISSPA_ERR_ARG;
+  int rmax = int((float)ri * 1.0f + 0.5);
+  if (rmax <= 0) rmax = nx / 2;
+  const float r2 = (float)(rmax * rmax);
+  int jmin = int(-rmax + 0.0f + 0.5), jmax = int(rmax + 0.0f + 0.5);
+  int imin = int(-rmax + 0.0f + 0.5), imax = int(rmax + 0.0f + 0.5);
+  jmin = std::max(jmin, -ny / 2);
+  jmax = std::min(jmax, ny / 2);
+  imin = std::max(imin, -nx / 2);
+  imax = std::min(imax, nx / 2);
+  const long long xy = (long long)nx * ny;
+#pragma omp parallel for schedule(dynamic)
+  for (int q = 0; q < n; ++q) {
+    const float alt = angles[3 * q], az = angles[3 * q + 1], phi = angles[3 * q + 2];
+    float m[9];
+    m[0] = (float)(cos((double)phi) * cos((double)az) - cos((double)alt) * sin((double)az) * sin((double)phi));
+    m[1] = (float)(-(sin((double)phi) * cos((double)az) + cos((double)alt) * sin((double)az) * cos((double)phi)));
+    m[2] = (float)(sin((double)alt) * sin((double)az));
+    m[3] = (float)(cos((double)phi) * sin((double)az) + cos((double)alt) * cos((double)az) * sin((double)phi));
+    m[4] = (float)(-sin((double)phi) * sin((double)az) + cos((double)alt) * cos((double)az) * cos((double)phi));
+    m[5] = (float)(-sin((double)alt) * cos((double)az));
+    m[6] = (float)(sin((double)alt) * sin((double)phi));
+    m[7] = (float)(sin((double)alt) * cos((double)phi));
+    m[8] = (float)cos((double)alt);
+    float* o = out + (size_t)q * xy;
+    std::fill(o, o + xy, 0.0f);
+    for (int k = -rmax; k < rmax; ++k) {
+      const float kz = (float)k;
+      for (int j = jmin; j < jmax; ++j) {
+        const float jy = (float)j;
+        for (int i = imin; i < imax; ++i) {
+          const float ix = (float)i;
+          if (r2 < ix * ix + jy * jy + kz * kz) continue;
+          const int x2 = (int)(m[0] * ix + m[1] * jy + m[2] * kz + (float)(nx / 2));
+          const int y2 = (int)(m[3] * ix + m[4] * jy + m[5] * kz + (float)(ny / 2));
+          const float z2 = m[6] * ix + m[7] * jy + m[8] * kz + (float)(nz / 2);
+          if (x2 < 0 || y2 < 0 || z2 < 0 || x2 >= nx - 1 || y2 >= ny - 1 || z2 >= nz - 1) continue;
+          const int z = (int)z2;
+          const float v = z2 - (float)z;
+          const long long ii = x2 + (long long)y2 * nx + (long long)z * xy;
+          const double s = (1.0 - (double)v) * (double)vol[ii] + (double)v * (double)vol[ii + xy];
+          o[(size_t)(j + ny / 2) * nx + i + nx / 2] += (float)s;
+        }
+      }
+    }
+  }
+  return GISSPA_OK;
+}
+
 }  // extern "C"

@@ -42,6 +42,7 @@ def load():
                                           C.c_int]
         lib.orc_tiles.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, C.c_int]
         lib.orc_num_threads.restype = C.c_int
+        lib.orc_project3d.argtypes = [_P, C.c_int, C.c_int, C.c_int, _P, C.c_int, C.c_int, _P]
         _lib = lib
     return _lib
 
@@ -128,6 +129,18 @@ def tiles(width: int, height: int, tile: int = 720):
     uly = np.zeros(4096, np.int32)
     n = load().orc_tiles(width, height, tile, ulx.ctypes.data, uly.ctypes.data, 4096)
     return list(zip(ulx[:n].tolist(), uly[:n].tolist()))
+
+
+def project3d(volume: np.ndarray, angles, ri: int = 0) -> np.ndarray:
+    """Projections [n][ny][nx] of a float32 volume [nz][ny][nx] at (alt, az, phi) radians
+    (emdata::project3d semantics; see orc_project3d)."""
+    vol = np.ascontiguousarray(volume, dtype=np.float32)
+    nz, ny, nx = vol.shape
+    ang = np.ascontiguousarray(np.asarray(angles, dtype=np.float32).reshape(-1, 3))
+    out = np.zeros((len(ang), ny, nx), dtype=np.float32)
+    st = load().orc_project3d(vol.ctypes.data, nx, ny, nz, ang.ctypes.data, len(ang), ri, out.ctypes.data)
+    assert st == 0, st
+    return out
 
 
 def num_threads() -> int:

@@ -71,3 +71,27 @@ def make_inputs(shape, n_templates: int, tsize: int, n_blobs: int, n_particles: 
         image[y:y + tsize, x:x + tsize] += amp * np.rot90(templates[j], q)
         parts[k] = (x + tsize // 2, y + tsize // 2, j, q)
     return image.astype(np.float32), templates.astype(np.float32), parts
+
+
+def bump_volume(size: int, n_blobs: int, seed: int) -> np.ndarray:
+    """float32 [size]^3 (z, y, x) sum of polynomial bumps a (1 - r^2/R^2)^2 with dyadic
+    centres (central 60 % of the box), radii 2..6 px and amplitudes 0.5..1."""
+    u = uniform(seed * 104729 + 3, n_blobs * 5).reshape(n_blobs, 5)
+    c = np.floor((0.2 + 0.6 * u[:, :3]) * size * 8) / 8
+    r = 2.0 + np.floor(u[:, 3] * 32) / 8
+    a = 0.5 + np.floor(u[:, 4] * 64) / 128
+    zz, yy, xx = np.mgrid[0:size, 0:size, 0:size].astype(np.float64)
+    vol = np.zeros((size, size, size), dtype=np.float64)
+    for (cx, cy, cz), rr, aa in zip(c, r, a):
+        q = ((xx - cx) * (xx - cx) + (yy - cy) * (yy - cy) + (zz - cz) * (zz - cz)) / (rr * rr)
+        vol += aa * np.where(q < 1.0, (1.0 - q) * (1.0 - q), 0.0)
+    return vol.astype(np.float32)
+
+
+# Projection cases: (volume size, blobs, seed, mask radius ri, angles (alt, az, phi) in radians,
+# dyadic so that they print and parse exactly).
+PROJECTION_CASES = {
+    "vol40": (40, 24, 5, 0, [(0.0, 0.0, 0.0), (0.5, 0.25, 1.0), (1.25, 2.5, 0.75), (2.0, 4.0, 5.5),
+                              (0.875, 3.125, 2.25), (3.0, 0.125, 6.0)]),
+    "vol33_ri12": (33, 16, 6, 12, [(0.375, 1.5, 0.5), (1.75, 5.25, 3.0), (2.625, 0.75, 4.5)]),
+}
