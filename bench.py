@@ -57,6 +57,8 @@ def args_parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host (cuda_graphs = 0), e.g. for per-launch profiling")
+    ap.add_argument("--shape", type=int, default=-1,
+                    help="with --batch: row-transform kernel shape (pass_b_shape) instead of the first")
     ap.add_argument("--batch", default=None,
                     help="D,E: fix templates x windows per correlation launch instead of autotuning (profiling)")
     ap.add_argument("--chosen", default="fp16_topk", choices=list(FORMS) + ["none"],
@@ -303,6 +305,7 @@ def main():
     params.update(FORMS[a.form])
     if a.batch:
         params["template_batch"], params["window_batch"] = (int(x) for x in a.batch.split(","))
+        params["pass_b_shape"] = a.shape
     if a.eager:
         params["cuda_graphs"] = 0
     cfg = gisspa.Config.default(**params)
