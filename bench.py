@@ -465,7 +465,8 @@ def main():
                "pairs_per_step": int(stats[-1].pairs), "picks_per_step": int(npicks),
                "stage_ms": {"prep": stats[-1].ms_prep, "sweep1": stats[-1].ms_sweep1,
                             "sweep2": stats[-1].ms_sweep2, "pick": stats[-1].ms_pick},
-               "gpu_launches": int(launches), "clocks": clk, "roofline": roofline, "e2e": e2e}
+               "gpu_launches": int(launches), "graph_replays": int(stats[-1].graph_replays), "clocks": clk,
+               "roofline": roofline, "e2e": e2e}
         if chosen is not None:
             res["chosen_form"] = chosen
         if world == 1 and not a.no_cpu_baseline:

@@ -620,7 +620,7 @@ void run_angles(Ctx& c, NormRun& r, int epi, int a0, int a1) {
   for (int a = a0 + 1; a < a1; ++a) GISSPA_CUDA(cudaGraphLaunch(g.exec, c.s));
   launch_counter() += g.launches * (a1 - a0 - 1);
   r.pairs += g.pairs * (a1 - a0 - 1);
-  h->graph_replays += a1 - a0 - 1;
+  h->st.graph_replays += a1 - a0 - 1;
 }
 
 // Sweep 1 (ComputeCCGSum norm.cu:523-544) or the single top-K sweep over angles [a0, a1).
@@ -1383,6 +1383,7 @@ int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx
     total.pairs_per_launch += h->st.pairs_per_launch / n;
     total.templates_per_launch += h->st.templates_per_launch / n;
     total.pass_samples += h->st.pass_samples;
+    total.graph_replays += h->st.graph_replays;
     total.window_size = h->st.window_size;
     all.insert(all.end(), one.begin(), one.end());
     offsets[i + 1] = all.size();

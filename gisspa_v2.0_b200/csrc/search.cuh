@@ -93,7 +93,6 @@ struct gisspa_handle {
   std::vector<gisspa::AngleGraph> graphs;
   gisspa::DevBuf angle_table, angle_cursor, angle_cur;
   bool capturing = false;
-  long long graph_replays = 0;
 
   gisspa_stats st{};
   std::map<long long, gisspa::TuneChoice> tuned;

@@ -122,6 +122,7 @@ typedef struct gisspa_stats {
   int window_size;
   int pass_b_variant;          /* pass B shape picked by the autotuner (last sweep) */
   double tuned_us_per_pair;    /* autotuner's measured time per pair of that shape */
+  long long graph_replays;     /* angles run as replays of a captured CUDA graph */
 } gisspa_stats;
 
 typedef struct gisspa_handle gisspa_handle;

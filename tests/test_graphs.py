@@ -37,3 +37,4 @@ def test_graph_replay_bit_identical(mode):
         assert stg.pairs == ste.pairs
         # replays count their captured kernels; the graph path adds one angle-select per replay
         assert stg.kernel_launches >= ste.kernel_launches
+        assert stg.graph_replays > 0 and ste.graph_replays == 0
