@@ -91,7 +91,8 @@ GRAD_DTYPE = np.dtype([(n, "<f4") for n in ("score", "d_dx", "d_dy", "d_theta", 
 
 class RunPaths(C.Structure):
     _fields_ = [("input", C.c_char * 1024), ("template_path", C.c_char * 1024), ("eulerfile", C.c_char * 1024),
-                ("output", C.c_char * 1024), ("first", C.c_int), ("last", C.c_int), ("gpu_id", C.c_int)]
+                ("output", C.c_char * 1024), ("first", C.c_int), ("last", C.c_int), ("gpu_id", C.c_int),
+                ("template_volume", C.c_char * 1024)]
 
 
 class Stats(C.Structure):

@@ -57,6 +57,7 @@ extern "C" int gisspa_config_load(const char* path, gisspa_config* cfg, gisspa_r
     // reference keys
     if (key == "input") copy_str(rp->input, val);
     else if (key == "template") copy_str(rp->template_path, val);
+    else if (key == "template_volume") copy_str(rp->template_volume, val);
     else if (key == "eulerfile") copy_str(rp->eulerfile, val);
     else if (key == "output") copy_str(rp->output, val);
     else if (key == "first") ok = parse_int(val, rp->first);

@@ -110,15 +110,25 @@ std::vector<std::pair<int, int>> work_intervals(int first, int last, int procs) 
   return r;
 }
 
-int run_device(int dev, const gisspa_config& cfg, const std::vector<float>& stack, int tw, int th, int nt,
-               const Euler& eu, const std::vector<LstEntry>& lst, int first, int last, std::string& out) {
+// Templates: a projected stack (tw x th x nt), or a 3D map (tw x th x td) projected on the
+// device at the angles in `angles` (nt triples, radians) when td > 0.
+struct TemplateSource {
+  std::vector<float> data;
+  int tw = 0, th = 0, td = 0;
+  std::vector<float> angles;
+};
+
+int run_device(int dev, const gisspa_config& cfg, const TemplateSource& ts, int nt, const Euler& eu,
+               const std::vector<LstEntry>& lst, int first, int last, std::string& out) {
   gisspa_handle* h = nullptr;
   int st = gisspa_create(&cfg, dev, &h);
   if (st) {
     std::fprintf(stderr, "device %d: %s\n", dev, gisspa_last_error(nullptr));
     return st;
   }
-  st = gisspa_set_templates(h, stack.data(), nt, tw, th);
+  st = ts.td > 0 ? gisspa_set_templates_from_volume(h, ts.data.data(), ts.tw, ts.th, ts.td, ts.angles.data(), nt, 0)
+                 : gisspa_set_templates(h, ts.data.data(), nt, ts.tw, ts.th);
+  if (st) std::fprintf(stderr, "device %d: %s\n", dev, gisspa_last_error(h));
   std::vector<gisspa_pick> picks(1 << 16);
   for (int i = first; i < last && !st; ++i) {
     const LstEntry& e = lst[i];
@@ -174,19 +184,33 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "empty micrograph list or Euler file\n");
     return 1;
   }
-  // Templates(path, count) (templates.cpp:11-31): count = number of Euler lines
-  std::vector<float> stack;
-  int tw = 0, th = 0;
-  for (int i = 0; i < nt; ++i) {
-    std::vector<float> one;
+  TemplateSource ts;
+  if (rp.template_volume[0]) {
+    // a 3D map projected on the device at the Euler file's angles (degrees -> radians with the
+    // reference's pi, utils/constants.h:3)
     int x, y, z;
-    if (!read_mrc(rp.template_path, i, one, x, y, z)) {
-      std::fprintf(stderr, "cannot read template %d of %s\n", i, rp.template_path);
+    if (!read_mrc(rp.template_volume, -1, ts.data, x, y, z) || z < 2) {
+      std::fprintf(stderr, "cannot read the 3D map %s\n", rp.template_volume);
       return 1;
     }
-    tw = x;
-    th = y;
-    stack.insert(stack.end(), one.begin(), one.end());
+    ts.tw = x;
+    ts.th = y / z;  // read_mrc stacks the sections: y holds ny * nz
+    ts.td = z;
+    for (int i = 0; i < nt; ++i)
+      for (float e : {eu.e1[i], eu.e2[i], eu.e3[i]}) ts.angles.push_back((float)((double)e * 3.1415926535 / 180.0));
+  } else {
+    // Templates(path, count) (templates.cpp:11-31): count = number of Euler lines
+    for (int i = 0; i < nt; ++i) {
+      std::vector<float> one;
+      int x, y, z;
+      if (!read_mrc(rp.template_path, i, one, x, y, z)) {
+        std::fprintf(stderr, "cannot read template %d of %s\n", i, rp.template_path);
+        return 1;
+      }
+      ts.tw = x;
+      ts.th = y;
+      ts.data.insert(ts.data.end(), one.begin(), one.end());
+    }
   }
   const int first = std::max(0, std::min(rp.first, (int)lst.size() - 1));
   const int last = std::min(rp.last, std::max(0, (int)lst.size()));
@@ -194,7 +218,7 @@ int main(int argc, char** argv) {
   int st = 0;
   if (rp.gpu_id != -1) {
     std::string out;
-    st = run_device(rp.gpu_id, cfg, stack, tw, th, nt, eu, lst, first, last, out);
+    st = run_device(rp.gpu_id, cfg, ts, nt, eu, lst, first, last, out);
     output << out;
   } else {
     int ndev = 0;
@@ -203,12 +227,12 @@ int main(int argc, char** argv) {
     const auto iv = work_intervals(first, last, ndev);
     std::vector<std::string> outs(iv.size());
     std::vector<int> sts(iv.size(), 0);
-    std::vector<std::thread> ts;
+    std::vector<std::thread> workers;
     for (size_t d = 0; d < iv.size(); ++d)
-      ts.emplace_back([&, d] {
-        sts[d] = run_device((int)d, cfg, stack, tw, th, nt, eu, lst, iv[d].first, iv[d].second, outs[d]);
+      workers.emplace_back([&, d] {
+        sts[d] = run_device((int)d, cfg, ts, nt, eu, lst, iv[d].first, iv[d].second, outs[d]);
       });
-    for (auto& t : ts) t.join();
+    for (auto& t : workers) t.join();
     for (size_t d = 0; d < iv.size(); ++d) {
       output << outs[d];
       if (sts[d]) st = sts[d];

@@ -106,6 +106,9 @@ typedef struct gisspa_run_paths {
   char eulerfile[1024];
   char output[1024];
   int first, last, gpu_id;
+  /* addition: a 3D map (MRC) to project into the templates on the GPU at the Euler file's
+     angles (alt, az, phi in degrees), instead of reading a projected stack from `template` */
+  char template_volume[1024];
 } gisspa_run_paths;
 
 /* Per-call timing and counters. */
