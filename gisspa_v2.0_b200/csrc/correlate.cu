@@ -138,14 +138,19 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   __shared__ __align__(8) uint64_t bars[2];
   // the row transform's table (length NZ) and the first NZ entries of the length-L table
   // used by the even/odd unpack, staged once: every row of every template reads them
-  __shared__ __align__(16) float2 tw_nz[NZ], tw_l[NZ];
+  __shared__ __align__(16) float2 tw_nz[NZ + NZ / 16], tw_l[NZ];
   for (int i = threadIdx.x; i < NZ; i += NW * 32) {
-    tw_nz[i] = __ldg(twNZ + i);
+    tw_nz[tw_pad_index(i)] = __ldg(twNZ + i);
     tw_l[i] = __ldg(twL + i);
   }
   const int team = threadIdx.x / TEAM, lt = threadIdx.x - team * TEAM;
   const int e = blockIdx.y, y0 = blockIdx.x * RB, win = a.b0 + e;
   const int angle = a.angle_state ? a.angle_state->index : a.angle;
+  // The correlation is the raw transform times 1/L^2, a power of two: scaling by it commutes
+  // exactly with float rounding (no overflow or underflow at these magnitudes), so the sums,
+  // the running maxima and the z-scores work on raw values and apply it once, bit for bit
+  // as if every value had been scaled first.
+  static_assert((L & (L - 1)) == 0, "window size a power of two");
   const float inv = 1.0f / (float)(L * L);
   const size_t wbase = (size_t)win * L * L;
   if (threadIdx.x == 0) {
@@ -195,8 +200,9 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const float4 m = *reinterpret_cast<const float4*>(a.musig + wbase + (size_t)oy * L + ox[i]);
-        ms[s][i][0] = make_float2(m.x, m.y);
-        ms[s][i][1] = make_float2(m.z, m.w);
+        // (mu L^2, (1/sigma) / L^2): z = (raw - mu L^2) (1/sigma) / L^2 = (c - mu) / sigma exactly
+        ms[s][i][0] = make_float2(m.x * (float)(L * L), m.y * inv);
+        ms[s][i][1] = make_float2(m.z * (float)(L * L), m.w * inv);
       }
     }
   }
@@ -254,7 +260,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         for (int i = 0; i < E; ++i)
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const float c = (h ? v[i].y : v[i].x) * inv;
+            const float c = h ? v[i].y : v[i].x;  // raw: the 1/L^2 is applied when folding
             acc1[s][i][h] += c;
             acc2[s][i][h] = fmaf(c, c, acc2[s][i][h]);
             if constexpr (EPI == EPI_TOPK) {
@@ -279,7 +285,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         for (int i = 0; i < E; ++i)
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
-            const float c = (h ? v[i].y : v[i].x) * inv;
+            const float c = h ? v[i].y : v[i].x;
             z[i][h] = (c - ms[s][i][h].x) * ms[s][i][h].y;
             zmax = fmaxf(zmax, z[i][h]);
           }
@@ -421,11 +427,11 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         const size_t pix = wbase + (size_t)oy * L + ox[i];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          atomicAdd(a.S1 + pix + h, (double)acc1[s][i][h]);
-          atomicAdd(a.S2 + pix + h, (double)acc2[s][i][h]);
+          atomicAdd(a.S1 + pix + h, (double)(acc1[s][i][h] * inv));
+          atomicAdd(a.S2 + pix + h, (double)(acc2[s][i][h] * (inv * inv)));
           if constexpr (EPI == EPI_TOPK) {
             if (barg[s][i][h] >= 0)
-              atomicMax(a.peak + pix + h, ((unsigned long long)float_key(best[s][i][h]) << 32) |
+              atomicMax(a.peak + pix + h, ((unsigned long long)float_key(best[s][i][h] * inv) << 32) |
                                               (unsigned)(0xFFFFFFFFu - (unsigned)barg[s][i][h]));
           }
         }

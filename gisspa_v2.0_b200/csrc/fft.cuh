@@ -104,10 +104,11 @@ struct TwGlobal {
   const float2* __restrict__ p;
   __device__ __forceinline__ float2 operator()(int i) const { return __ldg(p + i); }
 };
-struct TwShared {
-  const float2* p;
-  __device__ __forceinline__ float2 operator()(int i) const { return p[i]; }
+struct TwShared {  // staged with one pad entry per 16 (tw_pad_index): the strided reads of a
+  const float2* p;  // Stockham stage (indices 4k, k < 8) fall in distinct banks
+  __device__ __forceinline__ float2 operator()(int i) const { return p[i + (i >> 4)]; }
 };
+__host__ __device__ constexpr int tw_pad_index(int i) { return i + (i >> 4); }
 
 // Twiddle W_N^p for the stage (conjugated for the inverse transform).
 template <int SIGN, typename Tw>
