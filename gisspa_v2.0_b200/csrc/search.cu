@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "adjoint.cuh"
+#include "corr_generic.cuh"
 #include "correlate.cuh"
 #include "prep.cuh"
 #include "project.cuh"
@@ -48,8 +49,8 @@ int validate_config(const gisspa_config& c, std::string& err) {
     err = "window_size " + std::to_string(l) + " must be a positive multiple of 16";
     return GISSPA_ERR_SHAPE;
   }
-  if (!correlate_supported(l)) {
-    err = "window_size " + std::to_string(l) + " is not built (supported: 256, 512, 1024)";
+  if (l < 32 || l > 2048) {
+    err = "window_size " + std::to_string(l) + " outside [32, 2048]";
     return GISSPA_ERR_UNSUPPORTED;
   }
   if (c.overlap < 0 || c.overlap >= l) {
@@ -86,6 +87,10 @@ int validate_config(const gisspa_config& c, std::string& err) {
   }
   if (c.template_batch < 0 || c.window_batch < 0) {
     err = "template_batch and window_batch must be >= 0";
+    return GISSPA_ERR_ARG;
+  }
+  if (c.pass_b_shape >= 0 && !correlate_fast(l)) {
+    err = "pass_b_shape applies to window sizes with hand-tuned kernels (256, 512, 1024)";
     return GISSPA_ERR_ARG;
   }
   if (c.pass_b_shape < -1 || c.pass_b_shape >= correlate_variants(l)) {
@@ -384,12 +389,13 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
   gisspa_handle* h = c.h;
   const int l = c.l;
   int variant = 0;
-  if (h->cfg.template_batch > 0 && h->cfg.window_batch > 0 && h->cfg.pass_b_shape >= 0) {
+  const bool generic = !correlate_fast(l);  // no hand-tuned kernels for this window size
+  if (!generic && h->cfg.template_batch > 0 && h->cfg.window_batch > 0 && h->cfg.pass_b_shape >= 0) {
     if (!correlate_variant_ok(l, h->cfg.pass_b_shape, epi))
       throw CudaError{cudaErrorInvalidValue, "pass_b_shape not compiled for this window size and epilogue"};
     variant = h->cfg.pass_b_shape;
   }
-  if (h->cfg.template_batch == 0 && h->cfg.window_batch == 0) {
+  if (!generic && h->cfg.template_batch == 0 && h->cfg.window_batch == 0) {
     const long long key = (long long)l | ((long long)epi << 16) | ((long long)h->cfg.spectrum_precision << 24) |
                           ((long long)std::min(nt, 64) << 32) | ((long long)std::min(W, 64) << 40);
     auto it = h->tuned.find(key);
@@ -400,9 +406,17 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
     h->st.pass_b_variant = variant;
     h->st.tuned_us_per_pair = it->second.us_per_pair;
   }
-  float2* Q = buf<float2>(h->Q, (size_t)D * E * (l / 2) * l);
-  const float2* twL = h->fft.twiddles(l);
-  const float2* twNZ = h->fft.twiddles(l / 2);
+  float2* Q = nullptr;
+  const float2 *twL = nullptr, *twNZ = nullptr;
+  float2 *gz = nullptr, *gx = nullptr;
+  if (generic) {
+    gz = buf<float2>(h->gen_z, generic_z_elems(l, D * E));
+    gx = buf<float2>(h->gen_x, generic_x_elems(l, D * E));
+  } else {
+    Q = buf<float2>(h->Q, (size_t)D * E * (l / 2) * l);
+    twL = h->fft.twiddles(l);
+    twNZ = h->fft.twiddles(l / 2);
+  }
   args.err = h->dev_err.as<unsigned>();
   long long pairs = 0;
   for (int n0 = 0; n0 < nt; n0 += D) {
@@ -416,13 +430,16 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
       args.n0 = n0;
       args.D = d;
       cudaEvent_t* ev = nullptr;
-      if ((h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples && !h->capturing) {
+      if ((h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples && !h->capturing && !generic) {
         ev = h->sev[h->n_samples];
         h->sample_pairs[h->n_samples] = d * e;
         h->sample_d[h->n_samples] = d;
         ++h->n_samples;
       }
-      correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s, ev);
+      if (generic)
+        correlate_generic(cl, I, T, args, h->fft, gz, gx, c.s);
+      else
+        correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s, ev);
       pairs += (long long)d * e;
     }
   }
@@ -522,7 +539,8 @@ std::vector<unsigned char> angle_graph_key(Ctx& c, const NormRun& r, int epi) {
   for (const void* p : {(const void*)h->prep_real.as<void>(), (const void*)h->rot.as<void>(),
                         (const void*)h->rot_tmp.as<void>(), (const void*)h->rsums.as<void>(),
                         (const void*)h->tspec.as<void>(), (const void*)h->ispec.as<void>(),
-                        (const void*)h->Q.as<void>(), (const void*)a.S1, (const void*)a.S2, (const void*)a.peak,
+                        (const void*)h->Q.as<void>(), (const void*)h->gen_z.as<void>(),
+                        (const void*)h->gen_x.as<void>(), (const void*)a.S1, (const void*)a.S2, (const void*)a.peak,
                         (const void*)a.musig, (const void*)a.offx, (const void*)a.offy,
                         (const void*)a.cand, (const void*)a.cand_count, (const void*)h->dev_err.as<void>(),
                         (const void*)h->angle_table.as<void>(), (const void*)h->angle_cursor.as<void>(),
@@ -1175,9 +1193,12 @@ void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int n
   args.nt_total = ntm;
   args.err = buf<unsigned>(h->dev_err, 1);
   GISSPA_CUDA(cudaMemsetAsync(args.err, 0, sizeof(unsigned), c.s));
-  float2* Q = buf<float2>(h->Q, (size_t)ntm * (l / 2) * l);
-  const float2* twL = h->fft.twiddles(l);
-  const float2* twNZ = h->fft.twiddles(l / 2);
+  const bool generic = !correlate_fast(l);
+  float2* Q = generic ? nullptr : buf<float2>(h->Q, (size_t)ntm * (l / 2) * l);
+  const float2* twL = generic ? nullptr : h->fft.twiddles(l);
+  const float2* twNZ = generic ? nullptr : h->fft.twiddles(l / 2);
+  float2* gz = generic ? buf<float2>(h->gen_z, generic_z_elems(l, ntm)) : nullptr;
+  float2* gx = generic ? buf<float2>(h->gen_x, generic_x_elems(l, ntm)) : nullptr;
   // one launch per window: pair p = d covers template d of window b, written at [b][d]
   for (int b = 0; b < nw; ++b) {
     CorrLaunch cl{l, 1, ntm, spec, EPI_MAP};
@@ -1186,7 +1207,10 @@ void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int n
     args.n0 = 0;
     args.D = ntm;
     args.map_out = d_out + (size_t)b * ntm * c.L2;
-    correlate_launch(cl, static_cast<const float2*>(d_win), d_t, Q, args, twL, twNZ, c.s);
+    if (generic)
+      correlate_generic(cl, static_cast<const float2*>(d_win), d_t, args, h->fft, gz, gx, c.s);
+    else
+      correlate_launch(cl, static_cast<const float2*>(d_win), d_t, Q, args, twL, twNZ, c.s);
   }
   GISSPA_CUDA(cudaStreamSynchronize(c.s));
   unsigned flag = 0;

@@ -37,6 +37,15 @@ SMALL = {
                            defocus=1.7, dfdiff=0.1, dfang=30.0),
                       dict(angpix=1.0, phistep=90.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                            diameter=120.0, threshold=3.0, window_size=1024, overlap=512, norm_type=1)),
+    # the reference's default window size 320 (no hand-tuned kernels: the generic path), 2x2 windows
+    "norm_l320_w4": (dict(shape=(640, 640), n_particles=5, snr=0.6, n_templates=3, tsize=96, seed=25,
+                          defocus=1.6, dfdiff=0.05, dfang=20.0),
+                     dict(angpix=1.0, phistep=45.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                          diameter=70.0, threshold=3.0, window_size=320, overlap=0, norm_type=1)),
+    "nonorm_l320": (dict(shape=(800, 800), n_particles=6, snr=0.5, n_templates=3, tsize=96, seed=26,
+                         defocus=1.5, dfdiff=0.0, dfang=0.0),
+                    dict(angpix=1.0, phistep=60.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                         diameter=70.0, threshold=8.0, window_size=320, overlap=100, norm_type=0)),
     # norm_type=0 on 720^2 tiles of a 1024^2 micrograph with 512 windows (the tiled workload's geometry)
     "nonorm_l512": (dict(shape=(1024, 1024), n_particles=10, snr=0.5, n_templates=4, tsize=128, seed=23,
                          defocus=1.5, dfdiff=0.0, dfang=0.0),

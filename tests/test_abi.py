@@ -77,7 +77,8 @@ def test_format_pick_matches_reference_line():
 def test_create_rejects_bad_configs():
     lib = gisspa.load()
     h = C.c_void_p()
-    for over in [dict(window_size=300), dict(window_size=320), dict(phistep=0.0), dict(overlap=600),
+    for over in [dict(window_size=300), dict(window_size=16), dict(window_size=4096), dict(phistep=0.0),
+                 dict(overlap=600),
                  dict(pass_b_shape=9), dict(pass_b_shape=-2)]:
         cfg = gisspa.Config.default(angpix=1.0, phistep=5.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0,
                                     lowres=200.0, diameter=100.0, window_size=512, norm_type=1, **{})

@@ -89,6 +89,30 @@ def test_cc_maps_against_oracle(norm_case):
             assert rel_err(g[b, n], ref) < 1e-4, (b, n)
 
 
+def test_cc_maps_generic_window():
+    """Correlation maps at the reference's default window 320 (generic FFT path) against numpy."""
+    torch = pytest.importorskip("torch")
+    img, tmpl, ctf, cfg = small_case("norm_l320_w4")
+    s = gisspa.Searcher(cfg)
+    L = cfg.window_size
+    win = oracle.window_spectra(cfg, oracle.prep_image(cfg, ctf, img))[:2]
+    prep = oracle.prep_templates(cfg, ctf, tmpl)
+    T = np.stack([oracle.rotated_spectrum(cfg, ctf, prep[n], 30.0) for n in range(3)])
+    dW = torch.from_numpy(half_spectrum(win).astype(np.complex64)).cuda()
+    dT = torch.from_numpy(half_spectrum(T).astype(np.complex64)).cuda()
+    out = torch.zeros((2, 3, L, L), dtype=torch.float32, device="cuda")
+    lib = gisspa.load()
+    st = lib.gisspa_cc_maps(s.h, dW.data_ptr(), 2, dT.data_ptr(), 3, gisspa.SPEC_FP32, out.data_ptr())
+    assert st == 0, lib.gisspa_last_error(s.h)
+    g = out.cpu().numpy()
+    yy, xx = np.mgrid[0:L, 0:L]
+    chk = np.where((xx + yy) % 2 == 1, -1.0, 1.0)
+    for b in range(2):
+        for n in range(3):
+            ref = np.fft.ifft2(win[b] * np.conj(T[n]) * chk).real
+            assert rel_err(g[b, n], ref) < 1e-4, (b, n)
+
+
 def run_both(name, **over):
     img, tmpl, ctf, cfg = small_case(name)
     cfg = cfg.copy(**over)
@@ -99,7 +123,7 @@ def run_both(name, **over):
     return g, o, cfg, s
 
 
-@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4", "norm_l1024_w4"])
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4", "norm_l1024_w4", "norm_l320_w4"])
 def test_search_norm_chunk_picks(name):
     g, o, cfg, s = run_both(name)
     rep = compare_chunk_picks(g, o, cfg.threshold)
@@ -122,7 +146,7 @@ def test_search_norm_stats_maps():
     assert rel_err(sd_g, sd_o) < 1e-4
 
 
-@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l1024_w4"])
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l1024_w4", "norm_l320_w4"])
 def test_search_norm_topk(name):
     g, o, cfg, s = run_both(name, pick_mode=gisspa.PICK_TOPK, topk=20, exclusion_radius=30.0, threshold=2.0)
     assert len(o) > 0 and len(g) == len(o)
@@ -132,8 +156,9 @@ def test_search_norm_topk(name):
     assert np.allclose(np.sort(g["score"]), np.sort(o["score"]), rtol=SCORE_RTOL, atol=SCORE_ATOL)
 
 
-def test_search_nonorm():
-    g, o, cfg, s = run_both("nonorm_l512")
+@pytest.mark.parametrize("name", ["nonorm_l512", "nonorm_l320"])
+def test_search_nonorm(name):
+    g, o, cfg, s = run_both(name)
     rep = compare_template_picks(g, o, cfg.threshold)
     print("nonorm report", rep)
     assert len(o) > 0
