@@ -462,4 +462,17 @@ int gisspa_debug_wait_probe(gisspa_handle* h, double seconds) {
   });
 }
 
+int gisspa_debug_fft(gisspa_handle* h, void* data, long long rows, int n, int sign) {
+  if (!h) return GISSPA_ERR_ARG;
+  if (!data || rows < 0 || n < 1 || n > 16384 || (sign != -1 && sign != 1)) {
+    h->err = "debug_fft: data non-null, rows >= 0, 1 <= n <= 16384, sign -1 or +1";
+    return GISSPA_ERR_ARG;
+  }
+  return guarded(h, [&] {
+    GISSPA_CUDA(cudaSetDevice(h->device));
+    h->fft.rows(static_cast<float2*>(data), rows, n, sign, 1.f, h->stream);
+    GISSPA_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
 }  // extern "C"

@@ -2,7 +2,7 @@
 #include <cmath>
 #include <complex>
 
-#include "fft_generic.cuh"
+#include "fft_smooth.cuh"
 
 namespace gisspa {
 
@@ -43,6 +43,24 @@ __global__ void fft_pow2_rows_kernel(float2* __restrict__ data, long long nrows,
     __syncthreads();
   }
   for (int i = threadIdx.x; i < total; i += blockDim.x) base[i] = cscale(sm[i], scale);
+}
+
+// One or more rows of a length whose prime factors are 2, 3, 5 and 7 per CTA: load into
+// shared memory, Stockham stages, scaled store.
+template <int SIGN>
+__global__ void fft_smooth_rows_kernel(float2* __restrict__ data, long long nrows, int n, int rpc, SmoothPlan plan,
+                                       const float2* __restrict__ tw, float scale) {
+  extern __shared__ float2 sm[];
+  const long long row0 = (long long)blockIdx.x * rpc;
+  const int rows_here = (int)min((long long)rpc, nrows - row0);
+  float2* base = data + row0 * n;
+  float2* a = sm;
+  float2* b = sm + (size_t)rpc * n;
+  const int total = rows_here * n;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) a[i] = base[i];
+  __syncthreads();
+  a = smooth_stages<SIGN>(a, b, rows_here, n, n, plan, tw);
+  for (int i = threadIdx.x; i < total; i += blockDim.x) base[i] = cscale(a[i], scale);
 }
 
 __global__ void blue_pre_kernel(const float2* __restrict__ x, float2* __restrict__ a, long long rows, int n, int m,
@@ -117,6 +135,23 @@ void host_fft_pow2(std::vector<std::complex<double>>& x, int sign) {
 }
 
 }  // namespace
+
+SmoothPlan smooth_plan(int n) {
+  SmoothPlan p;
+  if (n < 2) return p;
+  int rest = n;
+  while (rest % 4 == 0 && rest > 4 && p.ns < SmoothPlan::kMax) {
+    p.r[p.ns++] = 4;
+    rest /= 4;
+  }
+  for (int f : {4, 2, 3, 5, 7})
+    while (rest % f == 0 && p.ns < SmoothPlan::kMax) {
+      p.r[p.ns++] = f;
+      rest /= f;
+    }
+  if (rest != 1) p.ns = 0;
+  return p;
+}
 
 const float2* FftEngine::twiddles(int n) {
   auto it = tw_.find(n);
@@ -194,6 +229,25 @@ void FftEngine::rows(float2* data, long long nrows, int n, int sign, float scale
       fft_pow2_rows_kernel<-1><<<(unsigned)grid, threads, smem, s>>>(data, nrows, n, logn, rpc, tw, scale);
     else
       fft_pow2_rows_kernel<1><<<(unsigned)grid, threads, smem, s>>>(data, nrows, n, logn, rpc, tw, scale);
+    GISSPA_LAUNCH_CHECK();
+    return;
+  }
+  const SmoothPlan sp = n <= kSmoothMax ? smooth_plan(n) : SmoothPlan{};
+  if (sp.ns > 0) {
+    const int rpc = n >= 2048 ? 1 : 2048 / n;
+    const size_t smem = 2 * sizeof(float2) * (size_t)rpc * n;
+    const float2* tw = twiddles(n);
+    const long long grid = (nrows + rpc - 1) / rpc;
+    if (smem > 48 * 1024) {
+      GISSPA_CUDA(cudaFuncSetAttribute(fft_smooth_rows_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+      GISSPA_CUDA(cudaFuncSetAttribute(fft_smooth_rows_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    }
+    if (sign < 0)
+      fft_smooth_rows_kernel<-1><<<(unsigned)grid, 256, smem, s>>>(data, nrows, n, rpc, sp, tw, scale);
+    else
+      fft_smooth_rows_kernel<1><<<(unsigned)grid, 256, smem, s>>>(data, nrows, n, rpc, sp, tw, scale);
     GISSPA_LAUNCH_CHECK();
     return;
   }

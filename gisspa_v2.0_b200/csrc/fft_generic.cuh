@@ -1,8 +1,10 @@
 // fft_generic.cuh — batched 1D/2D complex FFTs for every size outside the hot loop
 // (template and image preparation, window spectra, per-angle template spectra).
 //
-// Power-of-two lengths up to 16384 run one shared-memory transform per row; other
-// lengths use Bluestein's chirp-z algorithm on top of it.  2D transforms are
+// Power-of-two lengths up to 16384 run one shared-memory radix-2 transform per row; lengths
+// up to 8192 whose prime factors are 2, 3, 5 and 7 run one shared-memory mixed-radix
+// Stockham transform per row; other lengths use Bluestein's chirp-z algorithm on top of the
+// power-of-two transform.  2D transforms are
 // rows -> transpose -> rows (-> transpose).  All transforms are unnormalised.
 #pragma once
 
@@ -56,9 +58,20 @@ class DevBuf {
   size_t n_ = 0;
 };
 
+// Radices (4 first, then 2, 3, 5, 7) whose product is n; ns = 0 when n has a prime factor
+// above 7 (such lengths use Bluestein's algorithm).
+struct SmoothPlan {
+  static constexpr int kMax = 16;
+  int ns = 0;
+  int r[kMax] = {};
+};
+SmoothPlan smooth_plan(int n);
+// Longest row the mixed-radix kernel takes (two shared-memory copies of 8192 complex = 128 KB).
+constexpr int kSmoothMax = 8192;
+
 class FftEngine {
  public:
-  // Table of exp(-2 pi i p / n), p < n, n a power of two (device pointer, cached).
+  // Table of exp(-2 pi i p / n), p < n (device pointer, cached per n).
   const float2* twiddles(int n);
   // In-place transform of `rows` contiguous rows of length n (any n >= 1).
   void rows(float2* data, long long rows, int n, int sign, float scale, cudaStream_t s);

@@ -138,6 +138,7 @@ SIGNATURES = {
     "gisspa_shard_import": (C.c_int, [_P, _P, _P, _P]),
     "gisspa_shard_picks": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "gisspa_debug_wait_probe": (C.c_int, [_P, C.c_double]),
+    "gisspa_debug_fft": (C.c_int, [_P, _P, C.c_longlong, C.c_int, C.c_int]),
     "gisspa_project": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, C.c_int, _P]),
     "gisspa_set_templates_from_volume": (C.c_int, [_P, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, C.c_int]),
 }

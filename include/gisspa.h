@@ -308,6 +308,12 @@ int gisspa_debug_stage(gisspa_handle* h, int what, const float* image, int nx, i
  * never landed would; the handle stays usable. */
 int gisspa_debug_wait_probe(gisspa_handle* h, double seconds);
 
+/* In-place unnormalised 1D transform (sign -1 forward, +1 inverse) of `rows` contiguous
+ * complex rows of length n (1 <= n <= 16384) in DEVICE memory, through the library's generic
+ * FFT engine (the transforms of the preparation stages: radix 2, mixed radix 2/3/4/5/7 or
+ * Bluestein by length).  No counterpart in the reference, which calls cuFFT. */
+int gisspa_debug_fft(gisspa_handle* h, void* data, long long rows, int n, int sign);
+
 #ifdef __cplusplus
 }
 #endif
