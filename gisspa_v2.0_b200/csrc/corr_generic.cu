@@ -1,12 +1,14 @@
 // corr_generic.cu — the correlation and its epilogues for window sizes without hand-tuned
 // kernels.  Same results as pass A + pass B (correlate.cu) within FP32 rounding: the
-// transforms run on the generic FFT engine (radix-2 / Bluestein), the epilogues reproduce
+// transforms run in shared memory (mixed radix 2/3/4/5/7) in a fused two-pass form, or on the
+// generic FFT engine (Bluestein for other lengths) in an unfused form; the epilogues reproduce
 // pass B's per-pixel sums and maxima, chunk picks with the reference's tie order, norm_type=0
 // peaks and sums, and maps.  The reference's chunks are 256 consecutive pixels of the window's
 // linear index (norm.cu:583-597), so for L that is not a multiple of 256 they straddle rows:
-// the chunk kernels work on linear indices.
+// the chunk scans work on linear indices.
 #include "../../include/gisspa.h"
 #include "corr_generic.cuh"
+#include "fft_smooth.cuh"
 
 namespace gisspa {
 namespace {
@@ -179,17 +181,313 @@ __global__ void gen_map_kernel(const float2* __restrict__ X, CorrArgs a, int L) 
   a.map_out[(size_t)p * L2 + q] = gen_raw(X, p, L, oy, ox) / (float)L2;
 }
 
+// ---- fused two-pass form for window sizes whose prime factors are 2, 3, 5 and 7
+
+// Column pass: rows gr = p (L/2+1) + kx of the launch's half-spectrum products
+// I[b0 + e][kx][.] conj(T[n0 + d][kx][.]) (p = e D + d), each inverse-transformed along ky in
+// shared memory: Z[p][kx][y].
+template <typename SPEC>
+__global__ void gen_cols_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, int b0, int n0,
+                                int D, int L, long long nrows, int rpc, SmoothPlan plan, const float2* __restrict__ tw,
+                                float2* __restrict__ Z) {
+  extern __shared__ float2 sm[];
+  const int hz = L / 2 + 1;
+  const long long H = (long long)hz * L;
+  const long long row0 = (long long)blockIdx.x * rpc;
+  const int rows_here = (int)min((long long)rpc, nrows - row0);
+  float2* a = sm;
+  float2* b = sm + (size_t)rpc * L;
+  for (int i = threadIdx.x; i < rows_here * L; i += blockDim.x) {
+    const int r = i / L, k = i - r * L;
+    const long long gr = row0 + r;
+    const int p = (int)(gr / hz), kx = (int)(gr - (long long)p * hz);
+    const int e = p / D, d = p - e * D;
+    a[i] = cmulc(I[(size_t)(b0 + e) * H + (size_t)kx * L + k],
+                 SPEC::load(T + (size_t)(n0 + d) * H + (size_t)kx * L + k));
+  }
+  __syncthreads();
+  const float2* f = smooth_stages<1>(a, b, rows_here, L, L, plan, tw);
+  for (int i = threadIdx.x; i < rows_here * L; i += blockDim.x) Z[(size_t)row0 * L + i] = f[i];
+}
+
+// Row pass: one CTA per (block of RB window rows, window of the launch), over the launch's D
+// templates.  Window (state) row Y0 + r is transform row (Y0 + r + L/2) mod L, and state
+// column ox is transform column (ox + L/2) mod L (zero lag at (L/2, L/2)).  Rows r and
+// r + RB/2 are real, so their Hermitian spectra X_r[k] (= Z[p][k][y] for k <= L/2,
+// conj Z[p][L-k][y] above) go through one complex transform as X_r + i X_{r+RB/2}: the real
+// and imaginary parts of the result are the two rows.  Thread t holds the CTA's pixels
+// q = 256 i + t (state linear index Y0 L + q, q < RB L); for the chunk scans (EPI_CHUNK,
+// EPI_NONORM) RB L is a multiple of 256, so these are whole chunks of the reference's
+// 256-pixel scan and q = 256 i + t is pixel t of the CTA's chunk i.
+template <int EPI>
+__global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict__ Z, CorrArgs a, int L, int RB, int ld,
+                                                       SmoothPlan plan, const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  const int hr = RB / 2, npix = RB * L, nch = npix / 256, t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  float2* buf0 = sm;
+  float2* buf1 = sm + (size_t)hr * ld;
+  unsigned long long* red = reinterpret_cast<unsigned long long*>(sm + (size_t)2 * hr * ld);  // [nch][8]
+  double* dred = reinterpret_cast<double*>(red + (size_t)nch * 8);                            // [2][8]
+  char* st = reinterpret_cast<char*>(dred + 16);
+  const int e = blockIdx.y, win = a.b0 + e, Y0 = blockIdx.x * RB;
+  const long long L2 = (long long)L * L, H = (long long)(L / 2 + 1) * L;
+  const size_t wpix = (size_t)win * L2 + (size_t)Y0 * L;
+  const float inv = 1.0f / (float)L2;
+  const int angle = a.angle_state ? a.angle_state->index : a.angle;
+  float* s1 = reinterpret_cast<float*>(st);  // SUM / TOPK per-pixel accumulators
+  float* s2 = s1 + npix;
+  float* bst = s2 + npix;
+  int* barg = reinterpret_cast<int*>(bst + npix);
+  float2* ms = reinterpret_cast<float2*>(st);  // CHUNK: (mu, 1/sigma) of the CTA's pixels
+  if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+    for (int q = t; q < npix; q += 256) {
+      s1[q] = 0.f;
+      s2[q] = 0.f;
+      if constexpr (EPI == EPI_TOPK) {
+        bst[q] = -INFINITY;
+        barg[q] = -1;
+      }
+    }
+  }
+  if constexpr (EPI == EPI_CHUNK)
+    for (int q = t; q < npix; q += 256) ms[q] = a.musig[wpix + q];
+
+  for (int d = 0; d < a.D; ++d) {
+    const int p = e * a.D + d;
+    const float2* Zp = Z + (size_t)p * H;
+    for (int idx = t; idx < hr * L; idx += 256) {
+      const int k = idx / hr, r2 = idx - k * hr;
+      const int ya = (Y0 + r2 + L / 2) % L, yb = (Y0 + r2 + hr + L / 2) % L;
+      float2 A, B;
+      if (k <= L / 2) {
+        A = Zp[(size_t)k * L + ya];
+        B = Zp[(size_t)k * L + yb];
+      } else {
+        A = Zp[(size_t)(L - k) * L + ya];
+        B = Zp[(size_t)(L - k) * L + yb];
+        A.y = -A.y;
+        B.y = -B.y;
+      }
+      buf0[(size_t)r2 * ld + k] = make_float2(A.x - B.y, A.y + B.x);
+    }
+    __syncthreads();
+    const float2* f = smooth_stages<1>(buf0, buf1, hr, L, ld, plan, tw);
+
+    if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+      for (int q = t; q < npix; q += 256) {
+        const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+        const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+        const float c = (r < hr ? w.x : w.y) * inv;
+        s1[q] += c;
+        s2[q] = fmaf(c, c, s2[q]);
+        if constexpr (EPI == EPI_TOPK) {
+          if (c > bst[q]) {
+            bst[q] = c;
+            barg[q] = angle * a.nt_total + a.n0 + d;
+          }
+        }
+      }
+    } else if constexpr (EPI == EPI_CHUNK) {
+      bool hit = false;
+      for (int q = t; q < npix; q += 256) {
+        const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+        const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+        const float z = ((r < hr ? w.x : w.y) * inv - ms[q].x) * ms[q].y;
+        hit = hit || z >= a.thresh;
+      }
+      if (__syncthreads_or(hit)) {  // CTA-uniform
+        for (int i = 0; i < nch; ++i) {
+          const int q = 256 * i + t;
+          const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+          const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+          const float z = ((r < hr ? w.x : w.y) * inv - ms[q].x) * ms[q].y;
+          unsigned long long key = ((unsigned long long)float_key(z) << 32) | (unsigned)(255 - brev8(t));
+          for (int off = 16; off > 0; off >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+            key = o > key ? o : key;
+          }
+          if (lane == 0) red[i * 8 + wid] = key;
+        }
+        __syncthreads();
+        for (int i = t; i < nch; i += 256) {
+          unsigned long long best = 0;
+          for (int w = 0; w < 8; ++w) best = red[i * 8 + w] > best ? red[i * 8 + w] : best;
+          const float zb = key_float((uint32_t)(best >> 32));
+          if (!(zb >= a.thresh)) continue;
+          const int id = Y0 * L + i * 256 + brev8(255 - (unsigned)(best & 0xffu));
+          const int px = id % L, py = id / L;
+          const int cx = a.offx[win % a.bx] + px, cy = a.offy[win / a.bx] + py;
+          if (!(cx >= a.dmin && cx < a.nx - a.dmin && cy >= a.dmin && cy < a.ny - a.dmin)) continue;
+          const unsigned slot = atomicAdd(a.cand_count, 1u);
+          if (slot >= a.cand_cap) continue;
+          Cand cd;
+          cd.score = zb;
+          cd.x = px;
+          cd.y = py;
+          cd.window = win;
+          cd.templ = a.n0 + d;
+          cd.angle = angle;
+          cd.chunk = id >> 8;
+          cd.pad = 0;
+          a.cand[slot] = cd;
+        }
+      }
+    } else if constexpr (EPI == EPI_NONORM) {
+      double t1 = 0.0, t2 = 0.0;
+      for (int i = 0; i < nch; ++i) {
+        const int q = 256 * i + t;
+        const int r = q / L, ox = q - r * L, oy = Y0 + r, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+        const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+        const float v = r < hr ? w.x : w.y;
+        t1 += v;
+        t2 += (double)v * v;
+        float val = v;
+        if (ox < a.border || ox > L - a.border || oy < a.border || oy > L - a.border) val = 0.f;
+        unsigned long long key = ((unsigned long long)float_key(val) << 32) | (unsigned)(255 - brev8(t));
+        for (int off = 16; off > 0; off >>= 1) {
+          const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+          key = o > key ? o : key;
+        }
+        if (lane == 0) red[i * 8 + wid] = key;
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        t1 += __shfl_xor_sync(0xffffffffu, t1, off);
+        t2 += __shfl_xor_sync(0xffffffffu, t2, off);
+      }
+      if (lane == 0) {
+        dred[wid] = t1;
+        dred[8 + wid] = t2;
+      }
+      __syncthreads();
+      const size_t qq = (size_t)win * a.nt_total + a.n0 + d;
+      if (t == 0) {
+        double b1 = 0, b2 = 0;
+        for (int w = 0; w < 8; ++w) {
+          b1 += dred[w];
+          b2 += dred[8 + w];
+        }
+        atomicAdd(a.nn_sum + 2 * qq, b1);
+        atomicAdd(a.nn_sum + 2 * qq + 1, b2);
+      }
+      for (int i = t; i < nch; i += 256) {
+        unsigned long long best = 0;
+        for (int w = 0; w < 8; ++w) best = red[i * 8 + w] > best ? red[i * 8 + w] : best;
+        const float vb = key_float((uint32_t)(best >> 32));
+        if (vb > 0.f) {
+          const int chunk = Y0 * L / 256 + i;
+          const int tb = brev8(255 - (unsigned)(best & 0xffu));
+          atomicMax(a.nn_key + qq,
+                    ((unsigned long long)float_key(vb) << 32) | ((unsigned long long)(0xFFFFFu - chunk) << 8) | tb);
+        }
+      }
+    } else if constexpr (EPI == EPI_MAP) {
+      float* out = a.map_out + (size_t)p * L2 + (size_t)Y0 * L;
+      for (int q = t; q < npix; q += 256) {
+        const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+        const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+        out[q] = (r < hr ? w.x : w.y) * inv;
+      }
+    }
+    __syncthreads();  // the transform buffers and the reduction slots are rewritten next
+  }
+
+  if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+    for (int q = t; q < npix; q += 256) {
+      atomicAdd(a.S1 + wpix + q, (double)s1[q]);
+      atomicAdd(a.S2 + wpix + q, (double)s2[q]);
+      if constexpr (EPI == EPI_TOPK) {
+        if (barg[q] >= 0)
+          atomicMax(a.peak + wpix + q,
+                    ((unsigned long long)float_key(bst[q]) << 32) | (unsigned)(0xFFFFFFFFu - (unsigned)barg[q]));
+      }
+    }
+  }
+}
+
+// Rows per CTA of gen_rows_kernel: even, a divisor of L, about 2560 pixels per CTA, and for
+// the chunk scans (EPI_CHUNK, EPI_NONORM) RB L a multiple of 256; 0 when no such RB exists.
+int gen_rows_rb(int L, int epi) {
+  int rb0 = 1;
+  if (epi == EPI_CHUNK || epi == EPI_NONORM) {
+    int g = 256;
+    while (L % g) g >>= 1;
+    rb0 = 256 / g;
+  }
+  const int step = rb0 % 2 ? 2 * rb0 : rb0;
+  int rb = step;
+  while (rb * L < 2560 && rb + step <= L) rb += step;
+  while (rb <= L && L % rb) rb += step;
+  return rb <= L ? rb : 0;
+}
+
+size_t gen_rows_smem(int L, int RB, int epi) {
+  const size_t ld = (size_t)L + 1, npix = (size_t)RB * L, nch = npix / 256;
+  size_t b = sizeof(float2) * RB * ld + sizeof(unsigned long long) * nch * 8 + sizeof(double) * 16;
+  if (epi == EPI_SUM || epi == EPI_TOPK) b += 16 * npix;
+  if (epi == EPI_CHUNK) b += sizeof(float2) * npix;
+  return b;
+}
+
+constexpr size_t kGenSmemMax = 200 * 1024;
+
 }  // namespace
+
+bool generic_fused(int L, int epi) {
+  if (L > kSmoothMax || smooth_plan(L).ns == 0) return false;
+  const int rb = gen_rows_rb(L, epi);
+  return rb > 0 && gen_rows_smem(L, rb, epi) <= kGenSmemMax && (size_t)2 * sizeof(float2) * L <= kGenSmemMax;
+}
 
 bool correlate_fast(int L) { return L == 256 || L == 512 || L == 1024; }
 
 size_t generic_z_elems(int L, int P) { return (size_t)P * (L / 2 + 1) * L; }
-size_t generic_x_elems(int L, int P) { return (size_t)P * L * L; }
+size_t generic_x_elems(int L, int P, int epi) { return generic_fused(L, epi) ? 0 : (size_t)P * L * L; }
 
 void correlate_generic(const CorrLaunch& cl, const float2* I, const void* T, const CorrArgs& a, FftEngine& fft,
-                       float2* z, float2* x, cudaStream_t s) {
+                       float2* z, float2* x, cudaStream_t s, cudaEvent_t* ev) {
   const int L = cl.L, P = cl.E * cl.D;
   const long long H = (long long)(L / 2 + 1) * L, L2 = (long long)L * L;
+  if (ev) GISSPA_CUDA(cudaEventRecord(ev[0], s));
+  if (generic_fused(L, cl.epi)) {
+    const SmoothPlan plan = smooth_plan(L);
+    const float2* tw = fft.twiddles(L);
+    const long long nrows = (long long)P * (L / 2 + 1);
+    const int rpc = std::max(1, 2048 / L);
+    const size_t smc = 2 * sizeof(float2) * (size_t)rpc * L;
+    const unsigned gc = (unsigned)((nrows + rpc - 1) / rpc);
+    auto cols = [&](auto kernel, const auto* t) {
+      if (smc > 48 * 1024)
+        GISSPA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc));
+      kernel<<<gc, 256, smc, s>>>(I, t, a.b0, a.n0, cl.D, L, nrows, rpc, plan, tw, z);
+    };
+    switch (cl.spec) {
+      case GISSPA_SPEC_FP32: cols(gen_cols_kernel<SpecFp32>, static_cast<const float2*>(T)); break;
+      case GISSPA_SPEC_FP16: cols(gen_cols_kernel<SpecFp16>, static_cast<const __half2*>(T)); break;
+      case GISSPA_SPEC_BF16: cols(gen_cols_kernel<SpecBf16>, static_cast<const __nv_bfloat162*>(T)); break;
+      default: throw CudaError{cudaErrorInvalidValue, "unknown spectrum precision"};
+    }
+    GISSPA_LAUNCH_CHECK();
+    if (ev) GISSPA_CUDA(cudaEventRecord(ev[1], s));
+    const int rb = gen_rows_rb(L, cl.epi);
+    const size_t smr = gen_rows_smem(L, rb, cl.epi);
+    const dim3 gr((unsigned)(L / rb), (unsigned)cl.E);
+    auto rows = [&](auto kernel) {
+      if (smr > 48 * 1024)
+        GISSPA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr));
+      kernel<<<gr, 256, smr, s>>>(z, a, L, rb, L + 1, plan, tw);
+    };
+    switch (cl.epi) {
+      case EPI_SUM: rows(gen_rows_kernel<EPI_SUM>); break;
+      case EPI_TOPK: rows(gen_rows_kernel<EPI_TOPK>); break;
+      case EPI_CHUNK: rows(gen_rows_kernel<EPI_CHUNK>); break;
+      case EPI_NONORM: rows(gen_rows_kernel<EPI_NONORM>); break;
+      case EPI_MAP: rows(gen_rows_kernel<EPI_MAP>); break;
+      default: throw CudaError{cudaErrorInvalidValue, "unknown epilogue"};
+    }
+    GISSPA_LAUNCH_CHECK();
+    if (ev) GISSPA_CUDA(cudaEventRecord(ev[2], s));
+    return;
+  }
   const dim3 gp((unsigned)std::min(ceil_div(H, kT), 4096), (unsigned)P);
   switch (cl.spec) {
     case GISSPA_SPEC_FP32:
@@ -208,6 +506,7 @@ void correlate_generic(const CorrLaunch& cl, const float2* I, const void* T, con
   fft.rows(z, (long long)P * (L / 2 + 1), L, +1, 1.f, s);  // columns over ky
   gen_hermitian_rows_kernel<<<dim3((unsigned)std::min(ceil_div(L2, kT), 4096), (unsigned)P), kT, 0, s>>>(z, L, x);
   GISSPA_LAUNCH_CHECK();
+  if (ev) GISSPA_CUDA(cudaEventRecord(ev[1], s));
   fft.rows(x, (long long)P * L, L, +1, 1.f, s);  // rows over kx: real maps
   const unsigned chunks = (unsigned)(L2 / 256);  // L % 16 == 0 makes L^2 a multiple of 256
   switch (cl.epi) {
@@ -221,6 +520,7 @@ void correlate_generic(const CorrLaunch& cl, const float2* I, const void* T, con
     default: throw CudaError{cudaErrorInvalidValue, "unknown epilogue"};
   }
   GISSPA_LAUNCH_CHECK();
+  if (ev) GISSPA_CUDA(cudaEventRecord(ev[2], s));
 }
 
 }  // namespace gisspa

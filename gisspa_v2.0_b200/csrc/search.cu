@@ -411,7 +411,8 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
   float2 *gz = nullptr, *gx = nullptr;
   if (generic) {
     gz = buf<float2>(h->gen_z, generic_z_elems(l, D * E));
-    gx = buf<float2>(h->gen_x, generic_x_elems(l, D * E));
+    const size_t xe = generic_x_elems(l, D * E, epi);
+    gx = xe ? buf<float2>(h->gen_x, xe) : nullptr;
   } else {
     Q = buf<float2>(h->Q, (size_t)D * E * (l / 2) * l);
     twL = h->fft.twiddles(l);
@@ -430,14 +431,14 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
       args.n0 = n0;
       args.D = d;
       cudaEvent_t* ev = nullptr;
-      if ((h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples && !h->capturing && !generic) {
+      if ((h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples && !h->capturing) {
         ev = h->sev[h->n_samples];
         h->sample_pairs[h->n_samples] = d * e;
         h->sample_d[h->n_samples] = d;
         ++h->n_samples;
       }
       if (generic)
-        correlate_generic(cl, I, T, args, h->fft, gz, gx, c.s);
+        correlate_generic(cl, I, T, args, h->fft, gz, gx, c.s, ev);
       else
         correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s, ev);
       pairs += (long long)d * e;
@@ -1198,7 +1199,8 @@ void cc_maps(gisspa_handle* h, const void* d_win, int nw, const void* d_t, int n
   const float2* twL = generic ? nullptr : h->fft.twiddles(l);
   const float2* twNZ = generic ? nullptr : h->fft.twiddles(l / 2);
   float2* gz = generic ? buf<float2>(h->gen_z, generic_z_elems(l, ntm)) : nullptr;
-  float2* gx = generic ? buf<float2>(h->gen_x, generic_x_elems(l, ntm)) : nullptr;
+  const size_t xe = generic ? generic_x_elems(l, ntm, EPI_MAP) : 0;
+  float2* gx = xe ? buf<float2>(h->gen_x, xe) : nullptr;
   // one launch per window: pair p = d covers template d of window b, written at [b][d]
   for (int b = 0; b < nw; ++b) {
     CorrLaunch cl{l, 1, ntm, spec, EPI_MAP};

@@ -148,6 +148,10 @@ WORKLOADS = {
     # 8192^2, 1000 templates of 256^2, 5 deg, norm_type=1, 1024 windows overlap 256
     "whole_8192_t1000": dict(shape=(8192, 8192), n_particles=1000, snr=0.05, n_templates=1000, tsize=256, seed=5,
                              defocus=1.7, dfdiff=0.1, dfang=30.0),
+    # the 4096^2 workload at the reference's default window size 320 (overlap 120): window sizes
+    # without hand-tuned kernels
+    "whole_4096_t200_w320": dict(shape=(4096, 4096), n_particles=300, snr=0.05, n_templates=200, tsize=180, seed=2,
+                                 defocus=1.7, dfdiff=0.1, dfang=30.0),
     # profiling case: the 4096^2 workload's kernel shapes (512 windows, 180^2 templates) at 2048^2,
     # 24 templates, 4 angles
     "whole_2048_t24": dict(shape=(2048, 2048), n_particles=40, snr=0.05, n_templates=24, tsize=180, seed=3,
@@ -159,6 +163,8 @@ SEARCH_PARAMS = {
                           diameter=100.0, threshold=7.0, window_size=512, overlap=128, norm_type=0),
     "whole_4096_t200": dict(angpix=1.0, phistep=5.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                             diameter=140.0, threshold=7.0, window_size=512, overlap=192, norm_type=1),
+    "whole_4096_t200_w320": dict(angpix=1.0, phistep=5.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                                 diameter=140.0, threshold=7.0, window_size=320, overlap=120, norm_type=1),
     "whole_8192_t1000": dict(angpix=1.0, phistep=5.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                              diameter=200.0, threshold=7.0, window_size=1024, overlap=256, norm_type=1),
     # batching: uneven micrographs (batch_cases), 500 templates of 200^2, 3 degree step

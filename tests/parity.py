@@ -42,6 +42,20 @@ SMALL = {
                           defocus=1.6, dfdiff=0.05, dfang=20.0),
                      dict(angpix=1.0, phistep=45.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                           diameter=70.0, threshold=3.0, window_size=320, overlap=0, norm_type=1)),
+    # 336 = 2^4 3 7 (mixed-radix stages with radix 3 and 7, 16-row blocks for the chunk scans)
+    "norm_l336_w4": (dict(shape=(672, 672), n_particles=5, snr=0.6, n_templates=3, tsize=96, seed=27,
+                          defocus=1.6, dfdiff=0.05, dfang=20.0),
+                     dict(angpix=1.0, phistep=45.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                          diameter=70.0, threshold=3.0, window_size=336, overlap=0, norm_type=1)),
+    # 176 = 16 11: a prime factor above 7 (Bluestein transforms, the unfused generic form)
+    "norm_l176_w4": (dict(shape=(352, 352), n_particles=4, snr=0.6, n_templates=3, tsize=64, seed=28,
+                          defocus=1.6, dfdiff=0.05, dfang=20.0),
+                     dict(angpix=1.0, phistep=45.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                          diameter=50.0, threshold=3.0, window_size=176, overlap=0, norm_type=1)),
+    "nonorm_l176": (dict(shape=(800, 800), n_particles=6, snr=0.5, n_templates=3, tsize=64, seed=29,
+                         defocus=1.5, dfdiff=0.0, dfang=0.0),
+                    dict(angpix=1.0, phistep=60.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                         diameter=50.0, threshold=8.0, window_size=176, overlap=60, norm_type=0)),
     "nonorm_l320": (dict(shape=(800, 800), n_particles=6, snr=0.5, n_templates=3, tsize=96, seed=26,
                          defocus=1.5, dfdiff=0.0, dfang=0.0),
                     dict(angpix=1.0, phistep=60.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,

@@ -89,10 +89,12 @@ def test_cc_maps_against_oracle(norm_case):
             assert rel_err(g[b, n], ref) < 1e-4, (b, n)
 
 
-def test_cc_maps_generic_window():
-    """Correlation maps at the reference's default window 320 (generic FFT path) against numpy."""
+@pytest.mark.parametrize("name", ["norm_l320_w4", "norm_l336_w4", "norm_l176_w4"])
+def test_cc_maps_generic_window(name):
+    """Correlation maps at window sizes without hand-tuned kernels (the reference's default 320,
+    a mixed-radix 336 and a Bluestein 176) against numpy."""
     torch = pytest.importorskip("torch")
-    img, tmpl, ctf, cfg = small_case("norm_l320_w4")
+    img, tmpl, ctf, cfg = small_case(name)
     s = gisspa.Searcher(cfg)
     L = cfg.window_size
     win = oracle.window_spectra(cfg, oracle.prep_image(cfg, ctf, img))[:2]
@@ -123,7 +125,8 @@ def run_both(name, **over):
     return g, o, cfg, s
 
 
-@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4", "norm_l1024_w4", "norm_l320_w4"])
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4", "norm_l1024_w4", "norm_l320_w4", "norm_l336_w4",
+                                  "norm_l176_w4"])
 def test_search_norm_chunk_picks(name):
     g, o, cfg, s = run_both(name)
     rep = compare_chunk_picks(g, o, cfg.threshold)
@@ -146,7 +149,7 @@ def test_search_norm_stats_maps():
     assert rel_err(sd_g, sd_o) < 1e-4
 
 
-@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l1024_w4", "norm_l320_w4"])
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l1024_w4", "norm_l320_w4", "norm_l336_w4", "norm_l176_w4"])
 def test_search_norm_topk(name):
     g, o, cfg, s = run_both(name, pick_mode=gisspa.PICK_TOPK, topk=20, exclusion_radius=30.0, threshold=2.0)
     assert len(o) > 0 and len(g) == len(o)
@@ -156,7 +159,7 @@ def test_search_norm_topk(name):
     assert np.allclose(np.sort(g["score"]), np.sort(o["score"]), rtol=SCORE_RTOL, atol=SCORE_ATOL)
 
 
-@pytest.mark.parametrize("name", ["nonorm_l512", "nonorm_l320"])
+@pytest.mark.parametrize("name", ["nonorm_l512", "nonorm_l320", "nonorm_l176"])
 def test_search_nonorm(name):
     g, o, cfg, s = run_both(name)
     rep = compare_template_picks(g, o, cfg.threshold)
