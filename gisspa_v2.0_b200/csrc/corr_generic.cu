@@ -183,14 +183,32 @@ __global__ void gen_map_kernel(const float2* __restrict__ X, CorrArgs a, int L) 
 
 // ---- fused two-pass form for window sizes whose prime factors are 2, 3, 5 and 7
 
+// Rows per CTA of gen_rows_kernel: even, a divisor of L, about 1280 pixels per CTA, and for
+// the chunk scans (EPI_CHUNK, EPI_NONORM) RB L a multiple of 256; 0 when no such RB exists.
+__host__ __device__ constexpr int gen_rows_rb(int L, int epi) {
+  int rb0 = 1;
+  if (epi == EPI_CHUNK || epi == EPI_NONORM) {
+    int g = 256;
+    while (L % g) g >>= 1;
+    rb0 = 256 / g;
+  }
+  const int step = rb0 % 2 ? 2 * rb0 : rb0;
+  int rb = step;
+  while (rb * L < 1280 && rb + step <= L) rb += step;
+  while (rb <= L && L % rb) rb += step;
+  return rb <= L ? rb : 0;
+}
+
+
 // Column pass: rows gr = p (L/2+1) + kx of the launch's half-spectrum products
 // I[b0 + e][kx][.] conj(T[n0 + d][kx][.]) (p = e D + d), each inverse-transformed along ky in
 // shared memory: Z[p][kx][y].
-template <typename SPEC>
+template <int LC, typename SPEC>
 __global__ void gen_cols_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, int b0, int n0,
-                                int D, int L, long long nrows, int rpc, SmoothPlan plan, const float2* __restrict__ tw,
+                                int D, int L_, long long nrows, int rpc, SmoothPlan plan, const float2* __restrict__ tw,
                                 float2* __restrict__ Z) {
   extern __shared__ float2 sm[];
+  const int L = LC ? LC : L_;
   const int hz = L / 2 + 1;
   const long long H = (long long)hz * L;
   const long long row0 = (long long)blockIdx.x * rpc;
@@ -206,7 +224,7 @@ __global__ void gen_cols_kernel(const float2* __restrict__ I, const typename SPE
                  SPEC::load(T + (size_t)(n0 + d) * H + (size_t)kx * L + k));
   }
   __syncthreads();
-  const float2* f = smooth_stages<1>(a, b, rows_here, L, L, plan, tw);
+  const float2* f = smooth_stages_l<LC, 1>(a, b, rows_here, L, L, plan, tw);
   for (int i = threadIdx.x; i < rows_here * L; i += blockDim.x) Z[(size_t)row0 * L + i] = f[i];
 }
 
@@ -219,10 +237,13 @@ __global__ void gen_cols_kernel(const float2* __restrict__ I, const typename SPE
 // q = 256 i + t (state linear index Y0 L + q, q < RB L); for the chunk scans (EPI_CHUNK,
 // EPI_NONORM) RB L is a multiple of 256, so these are whole chunks of the reference's
 // 256-pixel scan and q = 256 i + t is pixel t of the CTA's chunk i.
-template <int EPI>
-__global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict__ Z, CorrArgs a, int L, int RB, int ld,
+template <int LC, int EPI>
+__global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict__ Z, CorrArgs a, int L_, int RB_,
                                                        SmoothPlan plan, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
+  constexpr int kRB = LC ? gen_rows_rb(LC, EPI) : 0;
+  static_assert(LC == 0 || kRB > 0, "no row block for LC");
+  const int L = LC ? LC : L_, RB = LC ? kRB : RB_, ld = L + 1;
   const int hr = RB / 2, npix = RB * L, nch = npix / 256, t = threadIdx.x, lane = t & 31, wid = t >> 5;
   float2* buf0 = sm;
   float2* buf1 = sm + (size_t)hr * ld;
@@ -271,7 +292,7 @@ __global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict_
       buf0[(size_t)r2 * ld + k] = make_float2(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
-    const float2* f = smooth_stages<1>(buf0, buf1, hr, L, ld, plan, tw);
+    const float2* f = smooth_stages_l<LC, 1>(buf0, buf1, hr, L, ld, plan, tw);
 
     if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
       for (int q = t; q < npix; q += 256) {
@@ -404,22 +425,6 @@ __global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict_
   }
 }
 
-// Rows per CTA of gen_rows_kernel: even, a divisor of L, about 2560 pixels per CTA, and for
-// the chunk scans (EPI_CHUNK, EPI_NONORM) RB L a multiple of 256; 0 when no such RB exists.
-int gen_rows_rb(int L, int epi) {
-  int rb0 = 1;
-  if (epi == EPI_CHUNK || epi == EPI_NONORM) {
-    int g = 256;
-    while (L % g) g >>= 1;
-    rb0 = 256 / g;
-  }
-  const int step = rb0 % 2 ? 2 * rb0 : rb0;
-  int rb = step;
-  while (rb * L < 2560 && rb + step <= L) rb += step;
-  while (rb <= L && L % rb) rb += step;
-  return rb <= L ? rb : 0;
-}
-
 size_t gen_rows_smem(int L, int RB, int epi) {
   const size_t ld = (size_t)L + 1, npix = (size_t)RB * L, nch = npix / 256;
   size_t b = sizeof(float2) * RB * ld + sizeof(unsigned long long) * nch * 8 + sizeof(double) * 16;
@@ -455,15 +460,23 @@ void correlate_generic(const CorrLaunch& cl, const float2* I, const void* T, con
     const int rpc = std::max(1, 2048 / L);
     const size_t smc = 2 * sizeof(float2) * (size_t)rpc * L;
     const unsigned gc = (unsigned)((nrows + rpc - 1) / rpc);
-    auto cols = [&](auto kernel, const auto* t) {
+    // L = 320, the reference's default window size, runs kernels compiled for that length
+    auto cols = [&](auto k320, auto kany, const auto* t) {
+      auto kernel = L == 320 ? k320 : kany;
       if (smc > 48 * 1024)
         GISSPA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc));
       kernel<<<gc, 256, smc, s>>>(I, t, a.b0, a.n0, cl.D, L, nrows, rpc, plan, tw, z);
     };
     switch (cl.spec) {
-      case GISSPA_SPEC_FP32: cols(gen_cols_kernel<SpecFp32>, static_cast<const float2*>(T)); break;
-      case GISSPA_SPEC_FP16: cols(gen_cols_kernel<SpecFp16>, static_cast<const __half2*>(T)); break;
-      case GISSPA_SPEC_BF16: cols(gen_cols_kernel<SpecBf16>, static_cast<const __nv_bfloat162*>(T)); break;
+      case GISSPA_SPEC_FP32:
+        cols(gen_cols_kernel<320, SpecFp32>, gen_cols_kernel<0, SpecFp32>, static_cast<const float2*>(T));
+        break;
+      case GISSPA_SPEC_FP16:
+        cols(gen_cols_kernel<320, SpecFp16>, gen_cols_kernel<0, SpecFp16>, static_cast<const __half2*>(T));
+        break;
+      case GISSPA_SPEC_BF16:
+        cols(gen_cols_kernel<320, SpecBf16>, gen_cols_kernel<0, SpecBf16>, static_cast<const __nv_bfloat162*>(T));
+        break;
       default: throw CudaError{cudaErrorInvalidValue, "unknown spectrum precision"};
     }
     GISSPA_LAUNCH_CHECK();
@@ -471,17 +484,18 @@ void correlate_generic(const CorrLaunch& cl, const float2* I, const void* T, con
     const int rb = gen_rows_rb(L, cl.epi);
     const size_t smr = gen_rows_smem(L, rb, cl.epi);
     const dim3 gr((unsigned)(L / rb), (unsigned)cl.E);
-    auto rows = [&](auto kernel) {
+    auto rows = [&](auto k320, auto kany) {
+      auto kernel = L == 320 ? k320 : kany;
       if (smr > 48 * 1024)
         GISSPA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr));
-      kernel<<<gr, 256, smr, s>>>(z, a, L, rb, L + 1, plan, tw);
+      kernel<<<gr, 256, smr, s>>>(z, a, L, rb, plan, tw);
     };
     switch (cl.epi) {
-      case EPI_SUM: rows(gen_rows_kernel<EPI_SUM>); break;
-      case EPI_TOPK: rows(gen_rows_kernel<EPI_TOPK>); break;
-      case EPI_CHUNK: rows(gen_rows_kernel<EPI_CHUNK>); break;
-      case EPI_NONORM: rows(gen_rows_kernel<EPI_NONORM>); break;
-      case EPI_MAP: rows(gen_rows_kernel<EPI_MAP>); break;
+      case EPI_SUM: rows(gen_rows_kernel<320, EPI_SUM>, gen_rows_kernel<0, EPI_SUM>); break;
+      case EPI_TOPK: rows(gen_rows_kernel<320, EPI_TOPK>, gen_rows_kernel<0, EPI_TOPK>); break;
+      case EPI_CHUNK: rows(gen_rows_kernel<320, EPI_CHUNK>, gen_rows_kernel<0, EPI_CHUNK>); break;
+      case EPI_NONORM: rows(gen_rows_kernel<320, EPI_NONORM>, gen_rows_kernel<0, EPI_NONORM>); break;
+      case EPI_MAP: rows(gen_rows_kernel<320, EPI_MAP>, gen_rows_kernel<0, EPI_MAP>); break;
       default: throw CudaError{cudaErrorInvalidValue, "unknown epilogue"};
     }
     GISSPA_LAUNCH_CHECK();

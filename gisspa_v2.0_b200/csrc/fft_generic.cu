@@ -136,23 +136,6 @@ void host_fft_pow2(std::vector<std::complex<double>>& x, int sign) {
 
 }  // namespace
 
-SmoothPlan smooth_plan(int n) {
-  SmoothPlan p;
-  if (n < 2) return p;
-  int rest = n;
-  while (rest % 4 == 0 && rest > 4 && p.ns < SmoothPlan::kMax) {
-    p.r[p.ns++] = 4;
-    rest /= 4;
-  }
-  for (int f : {4, 2, 3, 5, 7})
-    while (rest % f == 0 && p.ns < SmoothPlan::kMax) {
-      p.r[p.ns++] = f;
-      rest /= f;
-    }
-  if (rest != 1) p.ns = 0;
-  return p;
-}
-
 const float2* FftEngine::twiddles(int n) {
   auto it = tw_.find(n);
   if (it != tw_.end()) return it->second.as<float2>();

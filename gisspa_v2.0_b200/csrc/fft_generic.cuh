@@ -65,7 +65,24 @@ struct SmoothPlan {
   int ns = 0;
   int r[kMax] = {};
 };
-SmoothPlan smooth_plan(int n);
+__host__ __device__ constexpr SmoothPlan smooth_plan_c(int n) {
+  SmoothPlan p;
+  if (n < 2) return p;
+  const int fs[5] = {4, 2, 3, 5, 7};
+  int rest = n;
+  while (rest % 4 == 0 && rest > 4 && p.ns < SmoothPlan::kMax) {
+    p.r[p.ns++] = 4;
+    rest /= 4;
+  }
+  for (int i = 0; i < 5; ++i)
+    while (rest % fs[i] == 0 && p.ns < SmoothPlan::kMax) {
+      p.r[p.ns++] = fs[i];
+      rest /= fs[i];
+    }
+  if (rest != 1) p.ns = 0;
+  return p;
+}
+inline SmoothPlan smooth_plan(int n) { return smooth_plan_c(n); }
 // Longest row the mixed-radix kernel takes (two shared-memory copies of 8192 complex = 128 KB).
 constexpr int kSmoothMax = 8192;
 

@@ -65,6 +65,7 @@ template <int SIGN>
 __device__ __forceinline__ float2* smooth_stages(float2* a, float2* b, int rows, int n, int ld, const SmoothPlan& plan,
                                                  const float2* __restrict__ tw) {
   int Ns = 1;
+#pragma unroll
   for (int s = 0; s < plan.ns; ++s) {
     const int R = plan.r[s], m = n / R, nb = rows * m;
     for (int t = threadIdx.x; t < nb; t += blockDim.x) {
@@ -86,6 +87,20 @@ __device__ __forceinline__ float2* smooth_stages(float2* a, float2* b, int rows,
     Ns *= R;
   }
   return a;
+}
+
+// smooth_stages with the length and plan fixed at compile time when LC != 0 (the stage loop
+// unrolls and the index divisions become constant); LC = 0 takes n and plan at run time.
+template <int LC, int SIGN>
+__device__ __forceinline__ float2* smooth_stages_l(float2* a, float2* b, int rows, int n, int ld,
+                                                   const SmoothPlan& plan, const float2* __restrict__ tw) {
+  if constexpr (LC != 0) {
+    constexpr SmoothPlan kp = smooth_plan_c(LC);
+    static_assert(kp.ns > 0, "LC must factor into 2, 3, 5 and 7");
+    return smooth_stages<SIGN>(a, b, rows, LC, ld, kp, tw);
+  } else {
+    return smooth_stages<SIGN>(a, b, rows, n, ld, plan, tw);
+  }
 }
 
 }  // namespace gisspa
