@@ -1,6 +1,7 @@
 // common.cuh — shared device/host helpers for the B200 search library.
 #pragma once
 
+#include <mutex>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
@@ -36,6 +37,23 @@ long long& launch_counter();
     ++::gisspa::launch_counter();          \
     GISSPA_CUDA(cudaGetLastError());       \
   } while (0)
+
+// Runs f once per device for one kernel instance (cudaFuncSetAttribute acts on the current
+// device only, and one process may drive several GPUs from several threads).
+struct PerDeviceOnce {
+  std::mutex m;
+  unsigned long long done = 0;  // bit per device ordinal
+  template <typename F>
+  void operator()(F&& f) {
+    int dev = 0;
+    GISSPA_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(m);
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done & bit)) return;
+    f();
+    done |= bit;
+  }
+};
 
 // ---- complex arithmetic on float2 / double2
 // On sm_100 a complex add or subtract is one paired FP32 instruction ({add,sub}.f32x2 on the

@@ -435,6 +435,22 @@ size_t gen_rows_smem(int L, int RB, int epi) {
 
 constexpr size_t kGenSmemMax = 200 * 1024;
 
+// The row kernels of one epilogue (compiled for L = 320, and for any L): raises their dynamic
+// shared-memory limit to kGenSmemMax once per device, at the first launch that needs more
+// than the default 48 KB (the first angle of a sweep runs before any graph capture), and
+// returns the one for L.
+template <auto K320, auto KANY>
+auto gen_rows_pick(int L, size_t smem) {
+  if (smem > 48 * 1024) {
+    static PerDeviceOnce once;
+    once([] {
+      GISSPA_CUDA(cudaFuncSetAttribute(K320, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmemMax));
+      GISSPA_CUDA(cudaFuncSetAttribute(KANY, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmemMax));
+    });
+  }
+  return L == 320 ? K320 : KANY;
+}
+
 }  // namespace
 
 bool generic_fused(int L, int epi) {
@@ -461,10 +477,9 @@ void correlate_generic(const CorrLaunch& cl, const float2* I, const void* T, con
     const size_t smc = 2 * sizeof(float2) * (size_t)rpc * L;
     const unsigned gc = (unsigned)((nrows + rpc - 1) / rpc);
     // L = 320, the reference's default window size, runs kernels compiled for that length
+    // at most 2048 points per CTA: 32 KB, within the default shared-memory limit
     auto cols = [&](auto k320, auto kany, const auto* t) {
       auto kernel = L == 320 ? k320 : kany;
-      if (smc > 48 * 1024)
-        GISSPA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc));
       kernel<<<gc, 256, smc, s>>>(I, t, a.b0, a.n0, cl.D, L, nrows, rpc, plan, tw, z);
     };
     switch (cl.spec) {
@@ -484,18 +499,19 @@ void correlate_generic(const CorrLaunch& cl, const float2* I, const void* T, con
     const int rb = gen_rows_rb(L, cl.epi);
     const size_t smr = gen_rows_smem(L, rb, cl.epi);
     const dim3 gr((unsigned)(L / rb), (unsigned)cl.E);
-    auto rows = [&](auto k320, auto kany) {
-      auto kernel = L == 320 ? k320 : kany;
-      if (smr > 48 * 1024)
-        GISSPA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr));
-      kernel<<<gr, 256, smr, s>>>(z, a, L, rb, plan, tw);
-    };
+    auto rows = [&](auto kernel) { kernel<<<gr, 256, smr, s>>>(z, a, L, rb, plan, tw); };
     switch (cl.epi) {
-      case EPI_SUM: rows(gen_rows_kernel<320, EPI_SUM>, gen_rows_kernel<0, EPI_SUM>); break;
-      case EPI_TOPK: rows(gen_rows_kernel<320, EPI_TOPK>, gen_rows_kernel<0, EPI_TOPK>); break;
-      case EPI_CHUNK: rows(gen_rows_kernel<320, EPI_CHUNK>, gen_rows_kernel<0, EPI_CHUNK>); break;
-      case EPI_NONORM: rows(gen_rows_kernel<320, EPI_NONORM>, gen_rows_kernel<0, EPI_NONORM>); break;
-      case EPI_MAP: rows(gen_rows_kernel<320, EPI_MAP>, gen_rows_kernel<0, EPI_MAP>); break;
+      case EPI_SUM: rows(gen_rows_pick<gen_rows_kernel<320, EPI_SUM>, gen_rows_kernel<0, EPI_SUM>>(L, smr)); break;
+      case EPI_TOPK:
+        rows(gen_rows_pick<gen_rows_kernel<320, EPI_TOPK>, gen_rows_kernel<0, EPI_TOPK>>(L, smr));
+        break;
+      case EPI_CHUNK:
+        rows(gen_rows_pick<gen_rows_kernel<320, EPI_CHUNK>, gen_rows_kernel<0, EPI_CHUNK>>(L, smr));
+        break;
+      case EPI_NONORM:
+        rows(gen_rows_pick<gen_rows_kernel<320, EPI_NONORM>, gen_rows_kernel<0, EPI_NONORM>>(L, smr));
+        break;
+      case EPI_MAP: rows(gen_rows_pick<gen_rows_kernel<320, EPI_MAP>, gen_rows_kernel<0, EPI_MAP>>(L, smr)); break;
       default: throw CudaError{cudaErrorInvalidValue, "unknown epilogue"};
     }
     GISSPA_LAUNCH_CHECK();

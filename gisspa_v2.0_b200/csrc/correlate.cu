@@ -440,23 +440,6 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   }
 }
 
-// Runs f once per device for one kernel instance (cudaFuncSetAttribute acts on the current
-// device only, and one process may drive several GPUs from several threads).
-struct PerDeviceOnce {
-  std::mutex m;
-  unsigned long long done = 0;  // bit per device ordinal
-  template <typename F>
-  void operator()(F&& f) {
-    int dev = 0;
-    GISSPA_CUDA(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> g(m);
-    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
-    if (bit && (done & bit)) return;
-    f();
-    done |= bit;
-  }
-};
-
 // Launch with programmatic stream serialization (the kernel's griddep_wait orders it after
 // its predecessor).
 template <typename... P, typename... A>

@@ -1,6 +1,7 @@
 """CUDA-graph replay of the sweeps' angles (config cuda_graphs = 1, the default) against host
 launches of every kernel (cuda_graphs = 0): the same kernels in the same order, so picks and
-scores must be bit-identical, also after a size change forces a new capture."""
+scores must be bit-identical, also after a size change forces a new capture, for the hand-tuned
+and the generic correlation kernels."""
 import numpy as np
 import pytest
 
@@ -20,9 +21,12 @@ def _searchers(cfg, tmpl):
     return out
 
 
+# norm_l336_w4: a window size without hand-tuned kernels (the generic column / row kernels; its
+# chunk scan needs more than the default 48 KB of shared memory)
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l336_w4"])
 @pytest.mark.parametrize("mode", ["chunk", "topk"])
-def test_graph_replay_bit_identical(mode):
-    img, tmpl, ctf, cfg = small_case("norm_l256_w9")
+def test_graph_replay_bit_identical(name, mode):
+    img, tmpl, ctf, cfg = small_case(name)
     cfg = cfg.copy(phistep=30.0)  # 12 angles: 1 from the host, 11 replays per sweep
     if mode == "topk":
         cfg = cfg.copy(pick_mode=gisspa.PICK_TOPK, topk=40, exclusion_radius=20.0, threshold=2.0)
