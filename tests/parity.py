@@ -68,6 +68,49 @@ SMALL = {
 }
 
 
+def planted_copies_case():
+    """Known-answer input: three distinct band-limited random textures (64^2, inside a disk),
+    each planted once as an exact copy rotated by a multiple of 90 degrees (exact on the pixel
+    grid) at an integer offset, CTF-modulated, in unit noise.  Returns (image, templates, ctf,
+    config, truth) with truth rows (template, centre x, centre y, rotation in degrees); a
+    64-pixel template's centre lies between pixels (offset + 31.5)."""
+    rng = np.random.default_rng(7)
+    t, nt = 64, 3
+    yy, xx = np.mgrid[0:t, 0:t] - (t - 1) / 2
+    disk = (np.hypot(xx, yy) < 26).astype(np.float64)
+    ky = np.fft.fftfreq(t)[:, None]
+    kx = np.fft.fftfreq(t)[None, :]
+    lowpass = np.exp(-(kx ** 2 + ky ** 2) * (2 * np.pi * 1.5) ** 2 / 2)  # Gaussian blur, sigma 1.5 px
+    tmpl = np.stack([np.fft.ifft2(np.fft.fft2(rng.standard_normal((t, t))) * lowpass).real * disk
+                     for _ in range(nt)])
+    tmpl = (tmpl / tmpl.std(axis=(1, 2), keepdims=True)).astype(np.float32)
+    ny, nx = 512, 640
+    placed = [(1, 150, 170, 1), (0, 400, 130, 2), (2, 300, 380, 3)]  # template, x0, y0, quarter turns
+    clean = np.zeros((ny, nx))
+    for j, x0, y0, k in placed:
+        clean[y0:y0 + t, x0:x0 + t] += np.rot90(tmpl[j], k)
+    F = np.fft.rfft2(clean) * synth.ctf_2d(ny, nx, 1.0, 1.5, 0.0, 0.0)
+    img = (np.fft.irfft2(F, s=(ny, nx)) * 3.0 + rng.standard_normal((ny, nx))).astype(np.float32)
+    cfg = gisspa.Config.default(angpix=1.0, phistep=10.0, kk=3.0, energy=300.0, cs=2.7, highres=4.0, lowres=200.0,
+                                diameter=64.0, threshold=1.0, window_size=256, overlap=64, norm_type=1,
+                                pick_mode=gisspa.PICK_TOPK, topk=3, exclusion_radius=40.0)
+    truth = np.array([(j, x0 + (t - 1) / 2, y0 + (t - 1) / 2, 90.0 * k) for j, x0, y0, k in placed])
+    return img, tmpl, gisspa.Ctf(1.5, 0.0, 0.0), cfg, truth
+
+
+def assert_planted_copies_found(picks: np.ndarray, truth: np.ndarray):
+    """Each planted copy is one of the top picks: its template, its rotation (the reported
+    angle of a norm_type=1 pick is 360 - the search angle, norm.cu:654) and its centre within a
+    pixel."""
+    assert len(picks) == len(truth)
+    for j, cx, cy, ang in truth:
+        hit = [p for p in picks if p["template_id"] == int(j)]
+        assert len(hit) == 1, (j, picks)
+        p = hit[0]
+        assert abs(p["x"] - cx) <= 1.0 and abs(p["y"] - cy) <= 1.0, (j, p, cx, cy)
+        assert abs(((p["angle"] - ang) + 180.0) % 360.0 - 180.0) < 1e-3, (j, p, ang)
+
+
 def small_case(name: str):
     data, cfg = SMALL[name]
     c = synth.make_case(**data)

@@ -7,7 +7,7 @@ import pytest
 import gisspa
 import oracle
 import synth
-from parity import small_case
+from parity import assert_planted_copies_found, planted_copies_case, small_case
 
 
 @pytest.mark.parametrize("shape", [(8, 16), (64, 64), (30, 42), (7, 5), (1, 12), (256, 96)])
@@ -92,3 +92,9 @@ def test_oracle_search_runs_small():
     assert st.shape == (9, 256, 256, 2) and np.all(st[..., 1] > 0)
     order = np.lexsort((picks["chunk"], picks["template_id"], picks["window"], picks["angle_index"]))
     assert np.array_equal(order, np.arange(len(picks)))
+
+
+def test_oracle_finds_planted_copies():
+    """Known answer: rotated exact copies of three templates at their centres and rotations."""
+    img, tmpl, ctf, cfg, truth = planted_copies_case()
+    assert_planted_copies_found(oracle.search(cfg, ctf, img, tmpl), truth)
