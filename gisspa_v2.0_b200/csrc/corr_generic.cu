@@ -236,18 +236,20 @@ __global__ void gen_cols_kernel(const float2* __restrict__ I, const typename SPE
 // and imaginary parts of the result are the two rows.  Thread t holds the CTA's pixels
 // q = 256 i + t (state linear index Y0 L + q, q < RB L); for the chunk scans (EPI_CHUNK,
 // EPI_NONORM) RB L is a multiple of 256, so these are whole chunks of the reference's
-// 256-pixel scan and q = 256 i + t is pixel t of the CTA's chunk i.
+// 256-pixel scan and q = 256 i + t is pixel t of the CTA's chunk i.  The rows of up to TB
+// templates go through one transform pass (fewer block barriers, more butterflies per thread);
+// the epilogue then takes those templates in order.
 template <int LC, int EPI>
 __global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict__ Z, CorrArgs a, int L_, int RB_,
-                                                       SmoothPlan plan, const float2* __restrict__ tw) {
+                                                       int TB, SmoothPlan plan, const float2* __restrict__ tw) {
   extern __shared__ float2 sm[];
   constexpr int kRB = LC ? gen_rows_rb(LC, EPI) : 0;
   static_assert(LC == 0 || kRB > 0, "no row block for LC");
   const int L = LC ? LC : L_, RB = LC ? kRB : RB_, ld = L + 1;
   const int hr = RB / 2, npix = RB * L, nch = npix / 256, t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  float2* buf0 = sm;
-  float2* buf1 = sm + (size_t)hr * ld;
-  unsigned long long* red = reinterpret_cast<unsigned long long*>(sm + (size_t)2 * hr * ld);  // [nch][8]
+  float2* buf0 = sm;  // TB templates x hr complex rows, row stride ld
+  float2* buf1 = sm + (size_t)TB * hr * ld;
+  unsigned long long* red = reinterpret_cast<unsigned long long*>(sm + (size_t)2 * TB * hr * ld);  // [nch][8]
   double* dred = reinterpret_cast<double*>(red + (size_t)nch * 8);                            // [2][8]
   char* st = reinterpret_cast<char*>(dred + 16);
   const int e = blockIdx.y, win = a.b0 + e, Y0 = blockIdx.x * RB;
@@ -273,11 +275,12 @@ __global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict_
   if constexpr (EPI == EPI_CHUNK)
     for (int q = t; q < npix; q += 256) ms[q] = a.musig[wpix + q];
 
-  for (int d = 0; d < a.D; ++d) {
-    const int p = e * a.D + d;
-    const float2* Zp = Z + (size_t)p * H;
-    for (int idx = t; idx < hr * L; idx += 256) {
-      const int k = idx / hr, r2 = idx - k * hr;
+  for (int d0 = 0; d0 < a.D; d0 += TB) {
+    const int nd = min(TB, a.D - d0);
+    for (int idx = t; idx < nd * hr * L; idx += 256) {
+      const int g = idx / (hr * L), rem = idx - g * (hr * L);
+      const int k = rem / hr, r2 = rem - k * hr;
+      const float2* Zp = Z + (size_t)(e * a.D + d0 + g) * H;
       const int ya = (Y0 + r2 + L / 2) % L, yb = (Y0 + r2 + hr + L / 2) % L;
       float2 A, B;
       if (k <= L / 2) {
@@ -289,127 +292,134 @@ __global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict_
         A.y = -A.y;
         B.y = -B.y;
       }
-      buf0[(size_t)r2 * ld + k] = make_float2(A.x - B.y, A.y + B.x);
+      buf0[(size_t)(g * hr + r2) * ld + k] = make_float2(A.x - B.y, A.y + B.x);
     }
     __syncthreads();
-    const float2* f = smooth_stages_l<LC, 1>(buf0, buf1, hr, L, ld, plan, tw);
+    const float2* fg = smooth_stages_l<LC, 1>(buf0, buf1, nd * hr, L, ld, plan, tw);
 
-    if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
-      for (int q = t; q < npix; q += 256) {
-        const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
-        const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
-        const float c = (r < hr ? w.x : w.y) * inv;
-        s1[q] += c;
-        s2[q] = fmaf(c, c, s2[q]);
-        if constexpr (EPI == EPI_TOPK) {
-          if (c > bst[q]) {
-            bst[q] = c;
-            barg[q] = angle * a.nt_total + a.n0 + d;
+    // the group's templates in order, so every pixel folds them as the one-at-a-time sweep would
+    for (int g = 0; g < nd; ++g) {
+      const int d = d0 + g, p = e * a.D + d;
+      const float2* f = fg + (size_t)g * hr * ld;
+
+      if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+        for (int q = t; q < npix; q += 256) {
+          const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+          const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+          const float c = (r < hr ? w.x : w.y) * inv;
+          s1[q] += c;
+          s2[q] = fmaf(c, c, s2[q]);
+          if constexpr (EPI == EPI_TOPK) {
+            if (c > bst[q]) {
+              bst[q] = c;
+              barg[q] = angle * a.nt_total + a.n0 + d;
+            }
           }
         }
-      }
-    } else if constexpr (EPI == EPI_CHUNK) {
-      bool hit = false;
-      for (int q = t; q < npix; q += 256) {
-        const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
-        const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
-        const float z = ((r < hr ? w.x : w.y) * inv - ms[q].x) * ms[q].y;
-        hit = hit || z >= a.thresh;
-      }
-      if (__syncthreads_or(hit)) {  // CTA-uniform
-        for (int i = 0; i < nch; ++i) {
-          const int q = 256 * i + t;
+      } else if constexpr (EPI == EPI_CHUNK) {
+        bool hit = false;
+        for (int q = t; q < npix; q += 256) {
           const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
           const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
           const float z = ((r < hr ? w.x : w.y) * inv - ms[q].x) * ms[q].y;
-          unsigned long long key = ((unsigned long long)float_key(z) << 32) | (unsigned)(255 - brev8(t));
+          hit = hit || z >= a.thresh;
+        }
+        if (__syncthreads_or(hit)) {  // CTA-uniform
+          for (int i = 0; i < nch; ++i) {
+            const int q = 256 * i + t;
+            const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+            const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+            const float z = ((r < hr ? w.x : w.y) * inv - ms[q].x) * ms[q].y;
+            unsigned long long key = ((unsigned long long)float_key(z) << 32) | (unsigned)(255 - brev8(t));
+            for (int off = 16; off > 0; off >>= 1) {
+              const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+              key = o > key ? o : key;
+            }
+            if (lane == 0) red[i * 8 + wid] = key;
+          }
+          __syncthreads();
+          for (int i = t; i < nch; i += 256) {
+            unsigned long long best = 0;
+            for (int w = 0; w < 8; ++w) best = red[i * 8 + w] > best ? red[i * 8 + w] : best;
+            const float zb = key_float((uint32_t)(best >> 32));
+            if (!(zb >= a.thresh)) continue;
+            const int id = Y0 * L + i * 256 + brev8(255 - (unsigned)(best & 0xffu));
+            const int px = id % L, py = id / L;
+            const int cx = a.offx[win % a.bx] + px, cy = a.offy[win / a.bx] + py;
+            if (!(cx >= a.dmin && cx < a.nx - a.dmin && cy >= a.dmin && cy < a.ny - a.dmin)) continue;
+            const unsigned slot = atomicAdd(a.cand_count, 1u);
+            if (slot >= a.cand_cap) continue;
+            Cand cd;
+            cd.score = zb;
+            cd.x = px;
+            cd.y = py;
+            cd.window = win;
+            cd.templ = a.n0 + d;
+            cd.angle = angle;
+            cd.chunk = id >> 8;
+            cd.pad = 0;
+            a.cand[slot] = cd;
+          }
+        }
+      } else if constexpr (EPI == EPI_NONORM) {
+        double t1 = 0.0, t2 = 0.0;
+        for (int i = 0; i < nch; ++i) {
+          const int q = 256 * i + t;
+          const int r = q / L, ox = q - r * L, oy = Y0 + r, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+          const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+          const float v = r < hr ? w.x : w.y;
+          t1 += v;
+          t2 += (double)v * v;
+          float val = v;
+          if (ox < a.border || ox > L - a.border || oy < a.border || oy > L - a.border) val = 0.f;
+          unsigned long long key = ((unsigned long long)float_key(val) << 32) | (unsigned)(255 - brev8(t));
           for (int off = 16; off > 0; off >>= 1) {
             const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
             key = o > key ? o : key;
           }
           if (lane == 0) red[i * 8 + wid] = key;
         }
+        for (int off = 16; off > 0; off >>= 1) {
+          t1 += __shfl_xor_sync(0xffffffffu, t1, off);
+          t2 += __shfl_xor_sync(0xffffffffu, t2, off);
+        }
+        if (lane == 0) {
+          dred[wid] = t1;
+          dred[8 + wid] = t2;
+        }
         __syncthreads();
+        const size_t qq = (size_t)win * a.nt_total + a.n0 + d;
+        if (t == 0) {
+          double b1 = 0, b2 = 0;
+          for (int w = 0; w < 8; ++w) {
+            b1 += dred[w];
+            b2 += dred[8 + w];
+          }
+          atomicAdd(a.nn_sum + 2 * qq, b1);
+          atomicAdd(a.nn_sum + 2 * qq + 1, b2);
+        }
         for (int i = t; i < nch; i += 256) {
           unsigned long long best = 0;
           for (int w = 0; w < 8; ++w) best = red[i * 8 + w] > best ? red[i * 8 + w] : best;
-          const float zb = key_float((uint32_t)(best >> 32));
-          if (!(zb >= a.thresh)) continue;
-          const int id = Y0 * L + i * 256 + brev8(255 - (unsigned)(best & 0xffu));
-          const int px = id % L, py = id / L;
-          const int cx = a.offx[win % a.bx] + px, cy = a.offy[win / a.bx] + py;
-          if (!(cx >= a.dmin && cx < a.nx - a.dmin && cy >= a.dmin && cy < a.ny - a.dmin)) continue;
-          const unsigned slot = atomicAdd(a.cand_count, 1u);
-          if (slot >= a.cand_cap) continue;
-          Cand cd;
-          cd.score = zb;
-          cd.x = px;
-          cd.y = py;
-          cd.window = win;
-          cd.templ = a.n0 + d;
-          cd.angle = angle;
-          cd.chunk = id >> 8;
-          cd.pad = 0;
-          a.cand[slot] = cd;
+          const float vb = key_float((uint32_t)(best >> 32));
+          if (vb > 0.f) {
+            const int chunk = Y0 * L / 256 + i;
+            const int tb = brev8(255 - (unsigned)(best & 0xffu));
+            atomicMax(a.nn_key + qq,
+                      ((unsigned long long)float_key(vb) << 32) | ((unsigned long long)(0xFFFFFu - chunk) << 8) | tb);
+          }
+        }
+      } else if constexpr (EPI == EPI_MAP) {
+        float* out = a.map_out + (size_t)p * L2 + (size_t)Y0 * L;
+        for (int q = t; q < npix; q += 256) {
+          const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
+          const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
+          out[q] = (r < hr ? w.x : w.y) * inv;
         }
       }
-    } else if constexpr (EPI == EPI_NONORM) {
-      double t1 = 0.0, t2 = 0.0;
-      for (int i = 0; i < nch; ++i) {
-        const int q = 256 * i + t;
-        const int r = q / L, ox = q - r * L, oy = Y0 + r, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
-        const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
-        const float v = r < hr ? w.x : w.y;
-        t1 += v;
-        t2 += (double)v * v;
-        float val = v;
-        if (ox < a.border || ox > L - a.border || oy < a.border || oy > L - a.border) val = 0.f;
-        unsigned long long key = ((unsigned long long)float_key(val) << 32) | (unsigned)(255 - brev8(t));
-        for (int off = 16; off > 0; off >>= 1) {
-          const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
-          key = o > key ? o : key;
-        }
-        if (lane == 0) red[i * 8 + wid] = key;
-      }
-      for (int off = 16; off > 0; off >>= 1) {
-        t1 += __shfl_xor_sync(0xffffffffu, t1, off);
-        t2 += __shfl_xor_sync(0xffffffffu, t2, off);
-      }
-      if (lane == 0) {
-        dred[wid] = t1;
-        dred[8 + wid] = t2;
-      }
-      __syncthreads();
-      const size_t qq = (size_t)win * a.nt_total + a.n0 + d;
-      if (t == 0) {
-        double b1 = 0, b2 = 0;
-        for (int w = 0; w < 8; ++w) {
-          b1 += dred[w];
-          b2 += dred[8 + w];
-        }
-        atomicAdd(a.nn_sum + 2 * qq, b1);
-        atomicAdd(a.nn_sum + 2 * qq + 1, b2);
-      }
-      for (int i = t; i < nch; i += 256) {
-        unsigned long long best = 0;
-        for (int w = 0; w < 8; ++w) best = red[i * 8 + w] > best ? red[i * 8 + w] : best;
-        const float vb = key_float((uint32_t)(best >> 32));
-        if (vb > 0.f) {
-          const int chunk = Y0 * L / 256 + i;
-          const int tb = brev8(255 - (unsigned)(best & 0xffu));
-          atomicMax(a.nn_key + qq,
-                    ((unsigned long long)float_key(vb) << 32) | ((unsigned long long)(0xFFFFFu - chunk) << 8) | tb);
-        }
-      }
-    } else if constexpr (EPI == EPI_MAP) {
-      float* out = a.map_out + (size_t)p * L2 + (size_t)Y0 * L;
-      for (int q = t; q < npix; q += 256) {
-        const int r = q / L, ox = q - r * L, x = ox + L / 2 - (ox + L / 2 >= L ? L : 0);
-        const float2 w = f[(size_t)(r < hr ? r : r - hr) * ld + x];
-        out[q] = (r < hr ? w.x : w.y) * inv;
-      }
+      if constexpr (EPI == EPI_CHUNK || EPI == EPI_NONORM) __syncthreads();  // reduction slots reused next
     }
-    __syncthreads();  // the transform buffers and the reduction slots are rewritten next
+    __syncthreads();  // the transform buffers are rewritten next
   }
 
   if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
@@ -425,15 +435,23 @@ __global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict_
   }
 }
 
-size_t gen_rows_smem(int L, int RB, int epi) {
+size_t gen_rows_smem(int L, int RB, int epi, int tb) {
   const size_t ld = (size_t)L + 1, npix = (size_t)RB * L, nch = npix / 256;
-  size_t b = sizeof(float2) * RB * ld + sizeof(unsigned long long) * nch * 8 + sizeof(double) * 16;
+  size_t b = sizeof(float2) * tb * RB * ld + sizeof(unsigned long long) * nch * 8 + sizeof(double) * 16;
   if (epi == EPI_SUM || epi == EPI_TOPK) b += 16 * npix;
   if (epi == EPI_CHUNK) b += sizeof(float2) * npix;
   return b;
 }
 
 constexpr size_t kGenSmemMax = 200 * 1024;
+
+// Templates per transform pass of gen_rows_kernel: up to kGenTB as the shared memory allows.
+constexpr int kGenTB = 4;
+int gen_rows_tb(int L, int RB, int epi) {
+  int tb = kGenTB;
+  while (tb > 1 && gen_rows_smem(L, RB, epi, tb) > kGenSmemMax) tb /= 2;
+  return tb;
+}
 
 // The row kernels of one epilogue (compiled for L = 320, and for any L): raises their dynamic
 // shared-memory limit to kGenSmemMax once per device, at the first launch that needs more
@@ -456,7 +474,7 @@ auto gen_rows_pick(int L, size_t smem) {
 bool generic_fused(int L, int epi) {
   if (L > kSmoothMax || smooth_plan(L).ns == 0) return false;
   const int rb = gen_rows_rb(L, epi);
-  return rb > 0 && gen_rows_smem(L, rb, epi) <= kGenSmemMax && (size_t)2 * sizeof(float2) * L <= kGenSmemMax;
+  return rb > 0 && gen_rows_smem(L, rb, epi, 1) <= kGenSmemMax && (size_t)2 * sizeof(float2) * L <= kGenSmemMax;
 }
 
 bool correlate_fast(int L) { return L == 256 || L == 512 || L == 1024; }
@@ -497,9 +515,10 @@ void correlate_generic(const CorrLaunch& cl, const float2* I, const void* T, con
     GISSPA_LAUNCH_CHECK();
     if (ev) GISSPA_CUDA(cudaEventRecord(ev[1], s));
     const int rb = gen_rows_rb(L, cl.epi);
-    const size_t smr = gen_rows_smem(L, rb, cl.epi);
+    const int tb = gen_rows_tb(L, rb, cl.epi);
+    const size_t smr = gen_rows_smem(L, rb, cl.epi, tb);
     const dim3 gr((unsigned)(L / rb), (unsigned)cl.E);
-    auto rows = [&](auto kernel) { kernel<<<gr, 256, smr, s>>>(z, a, L, rb, plan, tw); };
+    auto rows = [&](auto kernel) { kernel<<<gr, 256, smr, s>>>(z, a, L, rb, tb, plan, tw); };
     switch (cl.epi) {
       case EPI_SUM: rows(gen_rows_pick<gen_rows_kernel<320, EPI_SUM>, gen_rows_kernel<0, EPI_SUM>>(L, smr)); break;
       case EPI_TOPK:
