@@ -3,6 +3,7 @@ reference config format and formats pick lines; no device is needed."""
 import ctypes as C
 import os
 import re
+import sys
 
 import numpy as np
 import pytest
@@ -103,3 +104,25 @@ def test_null_handle_new_entry_points():
     assert lib.gisspa_shard_export(None, None, None, None) == gisspa.ERR_ARG
     assert lib.gisspa_shard_picks(None, None, 0, C.byref(n)) == gisspa.ERR_ARG
     assert lib.gisspa_debug_wait_probe(None, 0.1) == gisspa.ERR_ARG
+
+
+def test_timing_script_writes_configs_the_reference_syntax_reads(tmp_path):
+    """oracle/ref_time.py hands the same config files to the reference build and to
+    gisspa_main: the library's parser (the reference's key syntax) reads back the workload."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref_time
+    import synth
+
+    wl = "whole_2048_t24"
+    d = str(tmp_path)
+    lst1, lst2 = ref_time.write_inputs(d, wl)
+    cfgp = os.path.join(d, "config")
+    ref_time.write_config(cfgp, wl, d, lst2, 2, os.path.join(d, "picks.txt"))
+    c, r = gisspa.load_config(cfgp)
+    want = synth.SEARCH_PARAMS[wl]
+    assert (c.window_size, c.overlap, c.norm_type) == (want["window_size"], want["overlap"], want["norm_type"])
+    assert (c.phistep, c.highres, c.lowres, c.diameter) == (want["phistep"], want["highres"], want["lowres"],
+                                                            want["diameter"])
+    assert (r.first, r.last, r.gpu_id) == (0, 2, 0) and r.input.decode() == lst2
+    with open(lst2) as fh:
+        assert sum(1 for ln in fh if ln.strip() and not ln.startswith("#")) == 2
