@@ -55,6 +55,8 @@ def args_parse():
     ap.add_argument("--form", default="plain", choices=list(FORMS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="--impl reference: skip timing the reference's own CUDA build beside the oracle")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host (cuda_graphs = 0), e.g. for per-launch profiling")
     ap.add_argument("--shape", type=int, default=-1,
@@ -179,6 +181,37 @@ def oracle_rate(case, cfg, n_angles: int):
     nt = case.templates.shape[0]
     mic_s = prep + per_rot * nt * n_angles
     return 1.0 / mic_s, oracle.num_threads(), sum(t), per_rot, prep
+
+
+def reference_cuda_timing(wl: str) -> dict:
+    """The reference's own CUDA build (its unmodified search sources, cuFFT, compiled for sm_100a
+    by oracle/ref_build.sh into oracle/_ref/gisspa_ref) beside this library's drop-in driver
+    gisspa_main on the same MRC / config / LST / Euler files of the workload, on this GPU: whole
+    process wall times for one and two micrographs, whose difference is the steady cost of one
+    micrograph (reference: norm.cu / nonorm.cu with cuFFT; ours: the C-ABI search)."""
+    ref_bin = os.path.join(REPO, "oracle", "_ref", "gisspa_ref")
+    ours_bin = os.path.join(REPO, "gisspa_v2.0_b200", "_build", "gisspa_main")
+    if not os.path.exists(ref_bin):
+        return {"unavailable": "oracle/_ref/gisspa_ref not built (the reference sources were absent at build time)"}
+    try:
+        import torch
+
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU visible"}
+    except Exception as e:  # noqa: BLE001
+        return {"unavailable": f"torch: {e}"}
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref_time
+
+    r = ref_time.time_binaries(wl, {"reference": ref_bin, "ours": ours_bin})
+    ref_s = r["reference"]["s_per_micrograph"]
+    ours_s = r["ours"]["s_per_micrograph"]
+    return {"value": 1.0 / ref_s, "unit": "micrographs/s", "s_per_micrograph": ref_s,
+            "s_setup": r["reference"]["s_setup"], "picks": r.get("reference_picks"),
+            "ours_gisspa_main": {"value": 1.0 / ours_s, "s_per_micrograph": ours_s, "s_setup": r["ours"]["s_setup"],
+                                 "picks": r.get("ours_picks")},
+            "speedup_per_micrograph": ref_s / ours_s,
+            "timing": "same B200, same files and config: t(2 micrographs) - t(1 micrograph), whole process"}
 
 
 # ------------------------------------------------------------------ batching workload
@@ -326,23 +359,30 @@ def main():
         if rank != 0:
             return
         case = synth.make_case(**data)
-        steps = []
+        steps, step_s = [], []
         for i in range(a.warmup + a.steps):
+            t0 = time.perf_counter()
             r = oracle_rate(case, cfg, angles)
             if i >= a.warmup:
                 steps.append(r)
+                step_s.append(time.perf_counter() - t0)
         rate = float(np.mean([s[0] for s in steps]))
         cores = steps[0][1]
         sample = (f"FP64 oracle, {wl}: 4 and 10 templates x 1 angle over all windows (both sweeps), "
                   f"extrapolated linearly to {data['n_templates']} templates x {angles} angles")
-        print(json.dumps({"impl": "reference", "metric": METRIC, "value": rate, "unit": "micrographs/s",
-                          "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
-                          "template_rotations_per_s": rate * data["n_templates"] * angles,
-                          "ms_per_step": 1000.0 / rate, "dtype": "f64", "data": "synthetic", "config": config_desc,
-                          "cpu_baseline": {"value": rate, "unit": "micrographs/s", "cores": cores, "kind": "port",
-                                           "sample": sample},
-                          "e2e": {"value": rate, "unit": "micrographs/s", "h2d_bytes_per_step": 0,
-                                  "d2h_bytes_per_step": 0}}))
+        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "micrographs/s",
+                "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
+                "template_rotations_per_s": rate * data["n_templates"] * angles,
+                "ms_per_step": 1000.0 * float(np.mean(step_s)),
+                "ms_per_step_is": "host wall time of one step's bounded sample (value is extrapolated from it)",
+                "extrapolated": True, "extrapolated_ms_per_micrograph": 1000.0 / rate,
+                "dtype": "f64", "data": "synthetic", "config": config_desc,
+                "cpu_baseline": {"value": rate, "unit": "micrographs/s", "cores": cores, "kind": "port",
+                                 "sample": sample, "extrapolated": True, "sample_s": float(np.mean(step_s))},
+                "e2e": {"value": rate, "unit": "micrographs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if not a.no_reference_cuda:
+            line["reference_cuda"] = reference_cuda_timing(wl)
+        print(json.dumps(line))
         return
 
     import torch
@@ -414,28 +454,34 @@ def main():
                "h2d_bytes_per_step": int(nx * ny * 4), "d2h_bytes_per_step": int(n_e2e * gisspa.PICK_DTYPE.itemsize),
                "timing": "host wall clock around the synchronous C-ABI call, max over ranks"}
 
-    # roofline of the correlation kernels (sampled CUDA-event durations inside the timed steps)
-    st_a = np.mean([x.pass_a_us for x in stats])
-    st_b = np.mean([x.pass_b_us for x in stats])
-    ppl = np.mean([x.pairs_per_launch for x in stats])
-    dpl = np.mean([x.templates_per_launch for x in stats])
+    # roofline of the dominant kernel: the correlation launch pair (pass A + pass B, which run
+    # back to back with programmatic dependent launch), timed by CUDA events around whole runs
+    # of launch pairs inside the timed steps (nothing recorded between the two passes)
+    t_pair = float(np.mean([x.corr_pair_us for x in stats]))
+    ppl = float(np.mean([x.pairs_per_launch for x in stats]))
+    dpl = float(np.mean([x.templates_per_launch for x in stats]))
     ba, bb = algorithmic_bytes(cfg.window_size, cfg.spectrum_precision, max(dpl, 1.0))
     peak, peak_kind = measured_peak_hbm()
-    kern = "pass_b" if st_b >= st_a else "pass_a"
-    dur = st_b if kern == "pass_b" else st_a
-    alg = (bb if kern == "pass_b" else ba) * ppl
-    achieved = alg / (dur * 1e-6) / 1e9 if dur > 0 else 0.0
+    alg = (ba + bb) * ppl
+    achieved = alg / (t_pair * 1e-6) / 1e9 if t_pair > 0 else 0.0
     tuned = cfg.window_size in (256, 512, 1024)
     # the committed per-pair DRAM bytes describe the hand-tuned kernels; window sizes without
-    # them run the generic column / row kernels (their samples bracket the same two halves)
-    tr = traffic_from_profiles(kern, cfg.spectrum_precision, ppl) if tuned else None
-    if not tuned:
-        kern = "generic_rows" if kern == "pass_b" else "generic_cols"
+    # them run the generic column / row kernels
+    tr = None
+    if tuned:
+        ta_ = traffic_from_profiles("pass_a", cfg.spectrum_precision, ppl)
+        tb_ = traffic_from_profiles("pass_b", cfg.spectrum_precision, ppl)
+        tr = ta_ + tb_ if ta_ is not None and tb_ is not None else None
+    kern = "pass_a+pass_b" if tuned else "generic_cols+generic_rows"
+    timed_pairs = int(sum(x.corr_timed_launches for x in stats))
     roofline = {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind, "traffic": tr,
-                "bytes_per_launch": alg, "launch_us": dur, "pass_a_us": st_a, "pass_b_us": st_b,
-                "pairs_per_launch": ppl, "templates_per_launch": dpl,
-                "pass_b_variant": int(stats[-1].pass_b_variant)}
+                "bytes_per_launch": alg, "bytes_per_pair": ba + bb, "launch_us": t_pair,
+                "pairs_per_launch": ppl, "templates_per_launch": dpl, "timed_launch_pairs": timed_pairs,
+                "launch_pairs_per_step": int(round(stats[-1].pairs / max(ppl, 1e-9))),
+                "pass_b_variant": int(stats[-1].pass_b_variant),
+                "timing": "CUDA events around each host-launched angle's run of launch pairs (first angle of "
+                          "each sweep), on the launching stream, inside the timed steps"}
 
     # the chosen form on the same micrograph: FP16 spectra, one top-K sweep (the numerator of
     # the target ratio against the plain FP32 two-sweep form timed above)
@@ -461,8 +507,8 @@ def main():
         v2 = world * a.steps / (float(t2.item()) / 1000.0)
         st2 = s2.stats()
         chosen = {"form": a.chosen, "value": v2, "unit": "micrographs/s", "ms_per_step": float(t2.item()) / a.steps,
-                  "vs_plain": v2 / value, "picks_per_step": int(n2), "pass_a_us": st2.pass_a_us,
-                  "pass_b_us": st2.pass_b_us}
+                  "vs_plain": v2 / value, "picks_per_step": int(n2), "launch_pair_us": st2.corr_pair_us,
+                  "pairs_per_launch": st2.pairs_per_launch}
         s2.close()
 
     res = None
@@ -484,7 +530,8 @@ def main():
             rate, cores, secs, per_rot, prep = oracle_rate(case, cfg, angles)
             res["cpu_baseline"] = {"value": rate, "unit": "micrographs/s", "cores": cores, "kind": "port",
                                    "sample": f"FP64 oracle, 4 and 10 templates x 1 angle over all windows "
-                                             f"({secs:.1f} s), extrapolated to the full workload"}
+                                             f"({secs:.1f} s), extrapolated to the full workload",
+                                   "extrapolated": True, "sample_s": secs}
         print(json.dumps(res))
     s.close()
     if world > 1:

@@ -89,6 +89,8 @@ int gisspa_create(const gisspa_config* cfg, int device, gisspa_handle** out) {
     for (auto& e : h->ev) GISSPA_CUDA(cudaEventCreate(&e));
     for (auto& r : h->sev)
       for (auto& e : r) GISSPA_CUDA(cudaEventCreate(&e));
+    for (auto& r : h->qev)
+      for (auto& e : r) GISSPA_CUDA(cudaEventCreate(&e));
   } catch (const CudaError& e) {
     g_create_error = std::string(cudaGetErrorString(e.code)) + " at " + e.where;
     delete h;

@@ -9,7 +9,9 @@
 // that every GPU loading the library holds until the process exits, and the call
 // makes no cudaMalloc, cudaFree or other allocating call.
 #include <cmath>
+#include <exception>
 #include <mutex>
+#include <string>
 
 #include "../../include/gisspa.h"
 #include "common.cuh"
@@ -24,7 +26,8 @@ static __device__ __align__(256) float2 g_noalloc_scratch[kNoAllocScratchBytes /
 // Twiddle tables exp(-2 pi i p / n) for n = 1024, 512, 256, 128, back to back.
 constexpr int kTwTotal = 1024 + 512 + 256 + 128;
 static __device__ __align__(256) float2 g_noalloc_twiddles[kTwTotal];
-// Set by a kernel whose bounded wait gave up; cleared by the call that reads it.
+// Set by a kernel whose bounded wait gave up.  Every call zeroes it on its stream before
+// its launches and reads it back after them.
 static __device__ unsigned g_noalloc_flag;
 
 int tw_offset(int n) { return n == 1024 ? 0 : n == 512 ? 1024 : n == 256 ? 1536 : 1792; }
@@ -71,6 +74,9 @@ int setup(int dev, std::string& err) {
       h[tw_offset(n) + k] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
   e = cudaMemcpy(s.twiddles, h, sizeof(h), cudaMemcpyHostToDevice);
+  // A copy from pageable memory may return before its DMA lands; a kernel on a caller's
+  // non-blocking stream would not be ordered after it, so wait for the device here (once).
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     err = std::string("twiddle upload: ") + cudaGetErrorString(e);
     return GISSPA_ERR_CUDA;
@@ -126,11 +132,27 @@ static int cc_maps_noalloc(const void* d_windows, int n_windows, const void* d_t
   args.map_out = d_out;
   args.err = ds.flag;
   CorrLaunch cl{L, n_windows, n_templates, spec, EPI_MAP, 0};
+  const cudaStream_t cs = static_cast<cudaStream_t>(stream);
   try {
+    // The flag keeps the previous call's value: clear it on this call's stream first.
+    GISSPA_CUDA(cudaMemsetAsync(ds.flag, 0, sizeof(unsigned), cs));
     correlate_launch(cl, static_cast<const float2*>(d_windows), d_templates, ds.scratch, args,
-                     ds.twiddles + tw_offset(L), ds.twiddles + tw_offset(L / 2), static_cast<cudaStream_t>(stream));
+                     ds.twiddles + tw_offset(L), ds.twiddles + tw_offset(L / 2), cs);
+    // A row kernel whose bounded wait for its slice of the intermediate gave up leaves its
+    // maps partly unwritten: wait for the launches and report that as a timeout.
+    GISSPA_CUDA(cudaStreamSynchronize(cs));
+    unsigned flag = 0;
+    GISSPA_CUDA(cudaMemcpy(&flag, ds.flag, sizeof(flag), cudaMemcpyDeviceToHost));
+    if (flag) {
+      err = "cc_maps_noalloc: a bounded wait inside the correlation kernels gave up (GPU overloaded or "
+            "stalled); the maps are incomplete";
+      return GISSPA_ERR_TIMEOUT;
+    }
   } catch (const CudaError& ce) {
     err = std::string(cudaGetErrorString(ce.code)) + " at " + ce.where;
+    return GISSPA_ERR_CUDA;
+  } catch (const std::exception& ex) {
+    err = std::string("cc_maps_noalloc: ") + ex.what();
     return GISSPA_ERR_CUDA;
   }
   return GISSPA_OK;
@@ -139,7 +161,13 @@ static int cc_maps_noalloc(const void* d_windows, int n_windows, const void* d_t
 extern "C" int gisspa_cc_maps_noalloc(const void* d_windows, int n_windows, const void* d_templates, int n_templates,
                                       int window_size, int spec, float* d_out, void* stream) {
   std::string err;
-  const int st = cc_maps_noalloc(d_windows, n_windows, d_templates, n_templates, window_size, spec, d_out, stream, err);
+  int st;
+  try {
+    st = cc_maps_noalloc(d_windows, n_windows, d_templates, n_templates, window_size, spec, d_out, stream, err);
+  } catch (...) {  // nothing may unwind through the C ABI
+    err = "cc_maps_noalloc: unexpected exception";
+    st = GISSPA_ERR_CUDA;
+  }
   if (st) set_handleless_error(err);
   return st;
 }

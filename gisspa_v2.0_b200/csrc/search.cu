@@ -421,7 +421,9 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
     twNZ = h->fft.twiddles(l / 2);
   }
   args.err = h->dev_err.as<unsigned>();
-  long long pairs = 0;
+  long long pairs = 0, launches = 0, dsum = 0;
+  const int seq = (!h->capturing && h->n_seqs < gisspa_handle::kSeqs) ? h->n_seqs++ : -1;
+  if (seq >= 0) GISSPA_CUDA(cudaEventRecord(h->qev[seq][0], c.s));
   for (int n0 = 0; n0 < nt; n0 += D) {
     const int d = std::min(D, nt - n0);
     for (int b0 = 0; b0 < W; b0 += E) {
@@ -433,7 +435,8 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
       args.n0 = n0;
       args.D = d;
       cudaEvent_t* ev = nullptr;
-      if ((h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples && !h->capturing) {
+      if (h->cfg.cuda_graphs == 0 && (h->launch_index++ & 15) == 0 && h->n_samples < gisspa_handle::kSamples &&
+          !h->capturing) {
         ev = h->sev[h->n_samples];
         h->sample_pairs[h->n_samples] = d * e;
         h->sample_d[h->n_samples] = d;
@@ -444,7 +447,15 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
       else
         correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s, ev);
       pairs += (long long)d * e;
+      dsum += d;
+      ++launches;
     }
+  }
+  if (seq >= 0) {
+    GISSPA_CUDA(cudaEventRecord(h->qev[seq][1], c.s));
+    h->seq_launches[seq] = launches;
+    h->seq_pairs[seq] = pairs;
+    h->seq_d[seq] = dsum;
   }
   return pairs;
 }
@@ -1257,6 +1268,7 @@ void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const giss
   const long long l0 = launch_counter();
   h->st = gisspa_stats{};
   h->n_samples = 0;
+  h->n_seqs = 0;
   h->launch_index = 0;
   unsigned* err = buf<unsigned>(h->dev_err, 1);
   GISSPA_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), c.s));
@@ -1299,6 +1311,22 @@ void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const giss
     h->st.templates_per_launch = dd / h->n_samples;
   }
   h->st.pass_samples = h->n_samples;
+  double tq = 0;
+  long long nl = 0, np = 0, nd = 0;
+  for (int i = 0; i < h->n_seqs; ++i) {
+    float q = 0;
+    GISSPA_CUDA(cudaEventElapsedTime(&q, h->qev[i][0], h->qev[i][1]));
+    tq += q;
+    nl += h->seq_launches[i];
+    np += h->seq_pairs[i];
+    nd += h->seq_d[i];
+  }
+  if (nl) {
+    h->st.corr_pair_us = 1000.0 * tq / (double)nl;
+    h->st.corr_timed_launches = nl;
+    h->st.pairs_per_launch = (double)np / (double)nl;
+    h->st.templates_per_launch = (double)nd / (double)nl;
+  }
 }
 
 // ---- sharded norm_type=1 search: one contiguous angle range per rank, state merged by the
@@ -1323,6 +1351,7 @@ void shard_begin(gisspa_handle* h, const float* d_img, int nx, int ny, const gis
   h->last_W = 0;
   h->st = gisspa_stats{};
   h->n_samples = 0;
+  h->n_seqs = 0;
   h->launch_index = 0;
   Ctx c = shard_ctx(h);
   unsigned* err = buf<unsigned>(h->dev_err, 1);

@@ -104,6 +104,11 @@ struct gisspa_handle {
   int sample_pairs[kSamples] = {}, sample_d[kSamples] = {};
   int n_samples = 0;
   long long launch_index = 0;
+  // events around whole runs of correlation launches (no event between the two passes)
+  static constexpr int kSeqs = 16;
+  cudaEvent_t qev[kSeqs][2] = {};
+  long long seq_launches[kSeqs] = {}, seq_pairs[kSeqs] = {}, seq_d[kSeqs] = {};
+  int n_seqs = 0;
 
   ~gisspa_handle() {
     for (auto& g : graphs)
@@ -111,6 +116,9 @@ struct gisspa_handle {
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
     for (auto& r : sev)
+      for (auto& e : r)
+        if (e) cudaEventDestroy(e);
+    for (auto& r : qev)
       for (auto& e : r)
         if (e) cudaEventDestroy(e);
     if (ev_in) cudaEventDestroy(ev_in);

@@ -101,7 +101,8 @@ class Stats(C.Structure):
                 ("kernel_launches", C.c_longlong), ("candidates", C.c_longlong), ("pass_a_us", C.c_double),
                 ("pass_b_us", C.c_double), ("pairs_per_launch", C.c_double), ("templates_per_launch", C.c_double),
                 ("pass_samples", C.c_int), ("window_size", C.c_int), ("pass_b_variant", C.c_int),
-                ("tuned_us_per_pair", C.c_double), ("graph_replays", C.c_longlong)]
+                ("tuned_us_per_pair", C.c_double), ("graph_replays", C.c_longlong), ("corr_pair_us", C.c_double),
+                ("corr_timed_launches", C.c_longlong)]
 
 
 class ShardInfo(C.Structure):

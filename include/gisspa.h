@@ -117,15 +117,21 @@ typedef struct gisspa_stats {
   long long pairs;            /* window x template x angle correlations evaluated */
   long long kernel_launches;  /* launches of this library's kernels in the last search */
   long long candidates;       /* picks found before the capacity check */
-  /* CUDA-event timing of a sample of correlation launches (every 16th launch pair) */
+  /* CUDA-event timing of a sample of correlation launches (every 16th launch pair), taken
+   * only with cuda_graphs = 0: an event between the two passes breaks their programmatic
+   * dependent launch overlap, so these split times are for profiling runs */
   double pass_a_us, pass_b_us; /* mean duration of one pass A / pass B launch */
-  double pairs_per_launch;     /* mean (window, template) pairs per sampled launch */
-  double templates_per_launch; /* mean template batch depth D of the sampled launches */
+  double pairs_per_launch;     /* mean (window, template) pairs per launch of the search */
+  double templates_per_launch; /* mean template batch depth D per launch of the search */
   int pass_samples;
   int window_size;
   int pass_b_variant;          /* pass B shape picked by the autotuner (last sweep) */
   double tuned_us_per_pair;    /* autotuner's measured time per pair of that shape */
   long long graph_replays;     /* angles run as replays of a captured CUDA graph */
+  /* CUDA events around whole runs of correlation launches (every host-launched angle: the
+   * first of each sweep when graphs are on), nothing recorded between them */
+  double corr_pair_us;         /* mean duration of one pass A + pass B launch pair */
+  long long corr_timed_launches; /* launch pairs inside those runs */
 } gisspa_stats;
 
 typedef struct gisspa_handle gisspa_handle;
@@ -226,11 +232,15 @@ int gisspa_cc_maps(gisspa_handle* h, const void* d_windows, int n_windows, const
  * 64 pairs at window_size 256, 16 at 512, 4 at 1024; larger calls return
  * GISSPA_ERR_CAPACITY with the reason in gisspa_last_error(NULL).  d_windows,
  * d_templates, d_out and window_size as for gisspa_cc_maps; runs on `stream`
- * (a cudaStream_t, NULL = default stream) of the current device.  The first call on
- * each device sets up that device's copy of the arrays (make that first call before
- * any stream capture).  Every call shares the one intermediate, which is fully
- * overwritten before it is read: calls that overlap on the GPU (other streams or
- * threads) race on it and must be serialised by the caller. */
+ * (a cudaStream_t, NULL = default stream) of the current device and returns once the
+ * maps are written (it waits for `stream`).  GISSPA_ERR_TIMEOUT: a bounded wait inside
+ * the kernels gave up and the maps are incomplete (the next call starts clean).  The
+ * first call on each device sets up that device's copy of the arrays (make that first
+ * call before any stream capture).  Every call shares the one intermediate and error
+ * flag, which keep the last call's contents; the intermediate is fully overwritten
+ * before it is read and the flag is cleared at the start of each call, so calls that
+ * overlap on the GPU (other streams or threads) race on them and must be serialised by
+ * the caller. */
 int gisspa_cc_maps_noalloc(const void* d_windows, int n_windows, const void* d_templates, int n_templates,
                            int window_size, int spec, float* d_out, void* stream);
 

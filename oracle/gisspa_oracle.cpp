@@ -27,6 +27,7 @@
 #include <cstring>
 #include <memory>
 #include <numeric>
+#include <map>
 #include <vector>
 
 #include "../include/gisspa.h"
@@ -111,19 +112,33 @@ struct Fft {
   }
 };
 
-// 2D transform of ny rows x nx columns (row-major), unnormalised.
+// Plans are cached per thread and length (building one costs as much as a few transforms).
+const Fft& plan(int n) {
+  thread_local std::map<int, std::unique_ptr<Fft>> cache;
+  std::unique_ptr<Fft>& p = cache[n];
+  if (!p) p = std::make_unique<Fft>(n);
+  return *p;
+}
+
+// 2D transform of ny rows x nx columns (row-major), unnormalised.  Columns are gathered in
+// groups of 16 (each row segment one contiguous read) and transformed one by one.
 void fft2(cd* d, int ny, int nx, int sign, bool parallel = true) {
-  Fft fr(nx), fc(ny);
+  const Fft& fr = plan(nx);
+  const Fft& fc = plan(ny);
+  constexpr int G = 16;
 #pragma omp parallel for schedule(static) if (parallel)
   for (int y = 0; y < ny; ++y) fr.exec(d + (size_t)y * nx, sign);
 #pragma omp parallel if (parallel)
   {
-    std::vector<cd> col(ny);
+    std::vector<cd> cols((size_t)G * ny);
 #pragma omp for schedule(static)
-    for (int x = 0; x < nx; ++x) {
-      for (int y = 0; y < ny; ++y) col[y] = d[(size_t)y * nx + x];
-      fc.exec(col.data(), sign);
-      for (int y = 0; y < ny; ++y) d[(size_t)y * nx + x] = col[y];
+    for (int x0 = 0; x0 < nx; x0 += G) {
+      const int g = std::min(G, nx - x0);
+      for (int y = 0; y < ny; ++y)
+        for (int q = 0; q < g; ++q) cols[(size_t)q * ny + y] = d[(size_t)y * nx + x0 + q];
+      for (int q = 0; q < g; ++q) fc.exec(cols.data() + (size_t)q * ny, sign);
+      for (int y = 0; y < ny; ++y)
+        for (int q = 0; q < g; ++q) d[(size_t)y * nx + x0 + q] = cols[(size_t)q * ny + y];
     }
   }
 }
@@ -483,6 +498,31 @@ void correlate(const cd* I, const cd* T, int l, double* out, std::vector<cd>& bu
   for (size_t i = 0; i < L2; ++i) out[i] = buf[i].real();
 }
 
+// Two correlation maps with one transform.  Z1 = I conj(T1) (-1)^(kx+ky) and Z2 likewise are
+// Hermitian (spectra of real images; the checkerboard is even for even l), so their inverse
+// transforms c1, c2 are real and IFFT(Z1 + i Z2) = c1 + i c2.  T2 = nullptr: c1 only.
+void correlate2(const cd* I, const cd* T1, const cd* T2, int l, double* out1, double* out2,
+                std::vector<cd>& buf) {
+  if (!T2) {
+    correlate(I, T1, l, out1, buf);
+    return;
+  }
+  const size_t L2 = (size_t)l * l;
+  buf.resize(L2);
+  const cd j(0, 1);
+  for (int y = 0; y < l; ++y)
+    for (int x = 0; x < l; ++x) {
+      size_t k = (size_t)y * l + x;
+      cd v = I[k] * std::conj(T1[k]) + j * (I[k] * std::conj(T2[k]));
+      buf[k] = ((x + y) & 1) ? -v : v;
+    }
+  fft2(buf.data(), l, l, +1, false);
+  for (size_t i = 0; i < L2; ++i) {
+    out1[i] = buf[i].real();
+    out2[i] = buf[i].imag();
+  }
+}
+
 inline unsigned brev8(unsigned v) {
   unsigned r = 0;
   for (int b = 0; b < 8; ++b) r |= ((v >> b) & 1u) << (7 - b);
@@ -642,13 +682,16 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
 #pragma omp parallel
     {
       std::vector<cd> buf;
-      std::vector<double> cc(L2);
+      std::vector<double> ccs(2 * L2);
 #pragma omp for schedule(dynamic)
       for (int b = 0; b < ws.W; ++b) {
         double* s1 = S1.data() + (size_t)b * L2;
         double* s2 = S2.data() + (size_t)b * L2;
         for (int n = 0; n < nts; ++n) {
-          correlate(ws.windows.data() + (size_t)b * L2, T.data() + (size_t)n * L2, l, cc.data(), buf);
+          if ((n & 1) == 0)
+            correlate2(ws.windows.data() + (size_t)b * L2, T.data() + (size_t)n * L2,
+                       n + 1 < nts ? T.data() + (size_t)(n + 1) * L2 : nullptr, l, ccs.data(), ccs.data() + L2, buf);
+          const double* cc = ccs.data() + (n & 1) * L2;
           for (size_t k = 0; k < L2; ++k) {
             double v = cc[k] / (double)L2;
             s1[k] += v;
@@ -685,12 +728,16 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
 #pragma omp parallel
       {
         std::vector<cd> buf;
-        std::vector<double> cc(L2);
+        std::vector<double> ccs(2 * L2);
 #pragma omp for schedule(dynamic)
         for (int b = 0; b < ws.W; ++b) {
           int i = b % ws.bx, j = b / ws.bx;
           for (int n = 0; n < nts; ++n) {
-            correlate(ws.windows.data() + (size_t)b * L2, T.data() + (size_t)n * L2, l, cc.data(), buf);
+            if ((n & 1) == 0)
+              correlate2(ws.windows.data() + (size_t)b * L2, T.data() + (size_t)n * L2,
+                         n + 1 < nts ? T.data() + (size_t)(n + 1) * L2 : nullptr, l, ccs.data(), ccs.data() + L2,
+                         buf);
+            const double* cc = ccs.data() + (n & 1) * L2;
             for (size_t ch = 0; ch < chunks; ++ch) {
               double best = 0;
               unsigned blane = 0;

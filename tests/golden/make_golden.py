@@ -11,6 +11,9 @@ reference binary exactly as its test script does (``main <config>``), parses the
 pick list it prints and stores ``<case>.json``: the case parameters, a checksum of
 the generated inputs and the reference's pick lines.  The Euler file gives
 template j the angles (j, 0, 0), so euler1 in each line identifies the template.
+norm_type=1 cases also store the pick lines of oracle/_ref/gisspa_ref_sync, the same
+sources with kernels.cu compiled for device debug (its warp-synchronous reduction tails
+then read what their neighbours wrote), as ``picks_sync``.
 """
 from __future__ import annotations
 
@@ -28,6 +31,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
 import fixture_data  # noqa: E402
+
+# Pick thresholds of the later cases, set from the oracle's score distribution so that each
+# case prints tens to hundreds of picks.
+THRESH = {"norm_1024_l512": 4.37, "norm_840_l320": 4.29, "nonorm_1024_l512_t8": 7.45, "nonorm_1024_l320": 12.9}
 
 # Cases satisfy the reference's preconditions: window_size % 16 == 0, windows <= templates
 # (norm.cu:141-147 reads past the stack otherwise) and images >= 720 for norm_type=0.
@@ -57,6 +64,43 @@ CASES = {
         outliers=[],
         cfg=dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, Highres=8.0, Lowres=200.0, diameter=64.0,
                  threshold=7.6, window_size=256, overlap=64, norm_type=0, invert=1, phase_flip=1)),
+    # the bench geometry's window (512, overlap 192: 3 x 3 windows on 1024^2)
+    "norm_1024_l512": dict(
+        data=dict(shape=(1024, 1024), n_templates=10, tsize=96, n_blobs=12, n_particles=8, amp=0.6, seed=15,
+                  margin=60),
+        ctf=dict(defocus=1.7, dfdiff=0.1, dfang=30.0),
+        outliers=[(900, 40, 22.0)],
+        cfg=dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, Highres=8.0, Lowres=200.0, diameter=80.0,
+                 threshold=THRESH["norm_1024_l512"], window_size=512, overlap=192, norm_type=1, invert=0,
+                 phase_flip=0)),
+    # the reference's default window 320 with overlap 120 (4 x 4 windows on 840^2)
+    "norm_840_l320": dict(
+        data=dict(shape=(840, 840), n_templates=16, tsize=48, n_blobs=10, n_particles=8, amp=0.6, seed=16,
+                  margin=40),
+        ctf=dict(defocus=1.5, dfdiff=0.05, dfang=60.0),
+        outliers=[],
+        cfg=dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, Highres=8.0, Lowres=200.0, diameter=40.0,
+                 threshold=THRESH["norm_840_l320"], window_size=320, overlap=120, norm_type=1, invert=0,
+                 phase_flip=0)),
+    # the tiled workload's geometry: 1024^2, 8 templates of 128^2, 10 degree steps, norm_type=0 in
+    # 720^2 tiles, 512 windows with 128 px overlap
+    "nonorm_1024_l512_t8": dict(
+        data=dict(shape=(1024, 1024), n_templates=8, tsize=128, n_blobs=16, n_particles=12, amp=0.5, seed=17,
+                  margin=60),
+        ctf=dict(defocus=1.5, dfdiff=0.0, dfang=0.0),
+        outliers=[],
+        cfg=dict(angpix=1.0, phistep=10.0, kk=3.0, energy=300.0, cs=2.7, Highres=8.0, Lowres=200.0, diameter=100.0,
+                 threshold=THRESH["nonorm_1024_l512_t8"], window_size=512, overlap=128, norm_type=0, invert=0,
+                 phase_flip=0)),
+    # the reference's defaults: norm_type=0, window 320, no overlap
+    "nonorm_1024_l320": dict(
+        data=dict(shape=(1024, 1024), n_templates=6, tsize=96, n_blobs=12, n_particles=10, amp=0.6, seed=18,
+                  margin=60),
+        ctf=dict(defocus=1.9, dfdiff=0.0, dfang=0.0),
+        outliers=[],
+        cfg=dict(angpix=1.0, phistep=30.0, kk=3.0, energy=300.0, cs=2.7, Highres=8.0, Lowres=200.0, diameter=70.0,
+                 threshold=THRESH["nonorm_1024_l320"], window_size=320, overlap=0, norm_type=0, invert=0,
+                 phase_flip=0)),
 }
 
 
@@ -142,16 +186,38 @@ def run_case(name: str, ref_bin: str, workdir: str) -> dict:
                 picks=[parse_line(ln) for ln in lines])
 
 
+def main_sync_only(a, wd):
+    """Adds to existing fixtures the pick list of the warp-safe test build (gisspa_ref_sync:
+    kernels.cu compiled with -G by oracle/ref_build.sh), keeping their reference picks."""
+    for name in a.cases:
+        path = os.path.join(a.out, f"{name}.json")
+        with open(path) as fh:
+            g = json.load(fh)
+        r = run_case(name, a.ref_sync, wd)
+        assert r["checksum"] == g["checksum"]
+        g["picks_sync"] = r["picks"]
+        with open(path, "w") as fh:
+            json.dump(g, fh, indent=0)
+        print(f"{name}: {len(r['picks'])} picks from the warp-safe build")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--ref", default=os.path.join(REPO, "oracle", "_ref", "gisspa_ref"))
+    ap.add_argument("--ref-sync", default=os.path.join(REPO, "oracle", "_ref", "gisspa_ref_sync"))
     ap.add_argument("--cases", nargs="*", default=list(CASES))
+    ap.add_argument("--sync-only", action="store_true",
+                    help="only add the warp-safe build's picks to existing fixtures")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     with tempfile.TemporaryDirectory() as wd:
+        if a.sync_only:
+            return main_sync_only(a, wd)
         for name in a.cases:
             res = run_case(name, a.ref, wd)
+            if CASES[name]["cfg"]["norm_type"] != 0 and os.path.exists(a.ref_sync):
+                res["picks_sync"] = run_case(name, a.ref_sync, wd)["picks"]
             with open(os.path.join(a.out, f"{name}.json"), "w") as fh:
                 json.dump(res, fh, indent=0)
             print(f"{name}: {res['n_picks']} reference picks")
