@@ -49,7 +49,7 @@ def args_parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="whole_4096_t200",
-                    choices=list(synth.WORKLOADS) + ["batch_c3", "project_c5"])
+                    choices=list(synth.WORKLOADS) + ["batch_c3", "project_c5", "adjoint_c4"])
     ap.add_argument("--batch-n", type=int, default=8,
                     help="batch_c3: micrographs per gisspa_search_batch call (the first n of the 32-micrograph batch)")
     ap.add_argument("--form", default="plain", choices=list(FORMS))
@@ -279,6 +279,76 @@ def bench_batch(a, rank: int, world: int, local: int):
         torch.distributed.destroy_process_group()
 
 
+# ------------------------------------------------------------------ differentiation workload
+def bench_adjoint(a, rank: int, local: int):
+    """Picks of the 4096^2 workload (200 templates of 180^2, 72 angles) with one top-K sweep
+    (K = 10,000, exclusion radius 16 px) in the FP32 and the BF16 template form; then per step,
+    for each form: the batched adjoint of all 10,000 picks (score and gradient in dx, dy, theta,
+    dfu, dfv, dfang; one call) and 20 steps of batched gradient-ascent refinement of the picks
+    and the micrograph CTF (one call).  The search itself is set-up, outside the timed region.
+    A sample of 32 picks is checked against central differences (h = 1e-3 px / degree) of the
+    library's own scores."""
+    import torch
+
+    torch.cuda.set_device(local)
+    wl = "whole_4096_t200"
+    case = synth.make_case(**synth.WORKLOADS[wl])
+    ctf = gisspa.Ctf(case.defocus, case.dfdiff, case.dfang)
+    res_forms = {}
+    for form, spec in (("fp32", gisspa.SPEC_FP32), ("bf16", gisspa.SPEC_BF16)):
+        params = dict(synth.SEARCH_PARAMS[wl])
+        params.update(spectrum_precision=spec, pick_mode=gisspa.PICK_TOPK, topk=10000, exclusion_radius=16.0,
+                      threshold=0.0)
+        s = gisspa.Searcher(gisspa.Config.default(**params), local)
+        s.set_templates(case.templates)
+        picks = s.search(case.image, ctf)
+        n = len(picks)
+        for _ in range(a.warmup):
+            s.score_grad(picks)
+        torch.cuda.synchronize()
+        tg, tr = [], []
+        for _ in range(a.steps):
+            t0 = time.perf_counter()
+            g = s.score_grad(picks)
+            tg.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            refined, c2, _ = s.refine(picks, steps=20, ctf=gisspa.Ctf(ctf.defocus, ctf.dfdiff, ctf.dfang))
+            tr.append(time.perf_counter() - t0)
+        # central differences of the library's scores on a sample of the picks
+        smp = picks[:: max(1, n // 32)][:32]
+        base = np.stack([np.full(len(smp), 0.21), np.full(len(smp), -0.17), smp["theta"] + 0.9], 1).astype(np.float32)
+        gb = s.score_grad(smp, base)
+        adj = np.stack([gb["d_dx"], gb["d_dy"], gb["d_theta"]], 1).astype(np.float64)
+        fd = np.zeros_like(adj)
+        for k in range(3):
+            d = np.zeros_like(base)
+            d[:, k] = 1e-3
+            hi, lo = base + d, base - d
+            step = hi[:, k].astype(np.float64) - lo[:, k].astype(np.float64)
+            fd[:, k] = (s.score_grad(smp, hi)["score"].astype(np.float64) -
+                        s.score_grad(smp, lo)["score"].astype(np.float64)) / step
+        rel = np.linalg.norm(adj - fd, axis=1) / np.maximum(np.linalg.norm(fd, axis=1), 1e-6)
+        res_forms[form] = {"picks": n, "grad_ms": 1000 * float(np.median(tg)), "refine20_ms": 1000 * float(np.median(tr)),
+                           "grad_picks_per_s": n / float(np.median(tg)),
+                           "refine_us_per_pick_step": 1e6 * float(np.median(tr)) / (20 * n),
+                           "mean_score_before": float(picks["score"].mean()),
+                           "mean_score_after": float(refined["score"].mean()),
+                           "ctf_after": [c2.defocus, c2.dfdiff, c2.dfang],
+                           "fd_check": {"picks": len(smp), "h": 1e-3, "median_rel": float(np.median(rel)),
+                                        "p90_rel": float(np.quantile(rel, 0.9)), "max_rel": float(rel.max())}}
+        s.close()
+    main = res_forms["fp32"]
+    res = {"metric": "picks/s of the batched adjoint (score + 6 gradients) on 10,000 picks", "value":
+           main["grad_picks_per_s"], "unit": "picks/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": main["grad_ms"] + main["refine20_ms"], "higher_is_better": True, "dtype": "f32 (f64 sums)",
+           "data": "synthetic (seeded Gaussian-blob projections planted in N(0,1) noise)",
+           "config": {"workload": "adjoint_c4", "picks_from": wl, "topk": 10000, "exclusion_radius": 16,
+                      "refine_steps": 20, "timing": "host wall clock around each synchronous C-ABI call"},
+           "forms": res_forms}
+    if rank == 0:
+        print(json.dumps(res))
+
+
 # ------------------------------------------------------------------ template generation workload
 def bench_project(a, rank: int, local: int):
     """One step = the 1000 projections of 256^2 that the 8192^2 workload searches, made from a
@@ -331,7 +401,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     wl = a.workload
-    if wl in ("batch_c3", "project_c5") and a.impl == "reference":
+    if wl in ("batch_c3", "project_c5", "adjoint_c4") and a.impl == "reference":
         if rank == 0:
             print(json.dumps({"impl": "reference", "unavailable": f"{wl}: the reference arm (the FP64 oracle on the "
                               "host cores) is timed on the single-micrograph workloads only"}))
@@ -340,6 +410,8 @@ def main():
         return bench_batch(a, rank, world, local)
     if wl == "project_c5":
         return bench_project(a, rank, local)
+    if wl == "adjoint_c4":
+        return bench_adjoint(a, rank, local)
     params = dict(synth.SEARCH_PARAMS[wl])
     params.update(FORMS[a.form])
     if a.batch:

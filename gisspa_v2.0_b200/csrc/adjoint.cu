@@ -18,7 +18,9 @@
 //   pick pixel.  Everything is recomputed from the prepared templates and the preprocessed
 //   micrograph; no spectrum of the search is stored.
 #include <cmath>
+#include <type_traits>
 
+#include "../../include/gisspa.h"
 #include "adjoint.cuh"
 
 namespace gisspa {
@@ -119,7 +121,7 @@ __global__ void window_sum_kernel(const float* __restrict__ img, int nx, int ny,
 
 // Bilinear sample with the reference's boundary rules (rotate_subIMG kernels.cu:557-579) and
 // its derivative in the sampling coordinates.
-__device__ __forceinline__ void bilinear(const float* __restrict__ img, int l, double x2, double y2, int& k0, int& k1,
+__device__ __forceinline__ void bilinear(int l, double x2, double y2, int& k0, int& k1,
                                          int& k2, int& k3, double& t, double& u, bool& inside) {
   inside = !(x2 < 0 || x2 > l - 1.0 || y2 < 0 || y2 > l - 1.0);
   if (!inside) return;
@@ -140,8 +142,26 @@ __device__ __forceinline__ void bilinear(const float* __restrict__ img, int l, d
   u = y2 - jj;
 }
 
-__global__ void __launch_bounds__(kGT) score_grad_kernel(GradArgs g, const GradPick* __restrict__ picks,
-                                                         float* __restrict__ out) {
+__device__ __forceinline__ double to_d(float v) { return (double)v; }
+__device__ __forceinline__ double to_d(__half v) { return (double)__half2float(v); }
+__device__ __forceinline__ double to_d(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
+
+template <typename V>
+__global__ void round_kernel(const float* __restrict__ in, long long n, V* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if constexpr (sizeof(V) == 2 && std::is_same<V, __half>::value)
+    out[i] = __float2half_rn(in[i]);
+  else
+    out[i] = __float2bfloat16_rn(in[i]);
+}
+
+// V: storage type of the prepared templates and their CTF derivatives (float, __half or
+// __nv_bfloat16); every sum is FP64 whatever the storage.
+template <typename V>
+__global__ void __launch_bounds__(kGT) score_grad_kernel(GradArgs g, const V* __restrict__ prep,
+                                                         const V* __restrict__ dprep,
+                                                         const GradPick* __restrict__ picks, float* __restrict__ out) {
   __shared__ double sh[kSums][kGT / 32];
   const GradPick pk = picks[blockIdx.x];
   const int L = g.L;
@@ -149,8 +169,8 @@ __global__ void __launch_bounds__(kGT) score_grad_kernel(GradArgs g, const GradP
   const double th = (double)pk.theta * kRefPi / 180.0;
   const double cs = cos(th), sn = sin(th);
   const double dm = 1.5 * g.d_m, r_in = dm / 2, r_out = dm / 2 + 2 * g.ehw;
-  const float* P = g.prep + (size_t)pk.n * L * L;
-  const float* D0 = g.dprep + (size_t)pk.n * L * L;
+  const V* P = prep + (size_t)pk.n * L * L;
+  const V* D0 = dprep + (size_t)pk.n * L * L;
   const size_t dstride = (size_t)g.nt * L * L;
   const int wx0 = g.offx[pk.b % g.bx], wy0 = g.offy[pk.b / g.bx];
   const double wscale = 1.0 / (L2 * (g.win_m[pk.b] != 0 ? g.win_m[pk.b] : 1.0));
@@ -176,17 +196,18 @@ __global__ void __launch_bounds__(kGT) score_grad_kernel(GradArgs g, const GradP
     int k0 = 0, k1 = 0, k2 = 0, k3 = 0;
     double t = 0, u = 0;
     bool inside;
-    bilinear(P, L, x2, y2, k0, k1, k2, k3, t, u, inside);
+    bilinear(L, x2, y2, k0, k1, k2, k3, t, u, inside);
     double R = 0, Rx = 0, Ry = 0, Dv[3] = {0, 0, 0};
     if (inside) {
-      const double p0 = P[k0], p1 = P[k1], p2 = P[k2], p3 = P[k3];
+      const double p0 = to_d(P[k0]), p1 = to_d(P[k1]), p2 = to_d(P[k2]), p3 = to_d(P[k3]);
       R = p0 * (1 - t) * (1 - u) + p1 * t * (1 - u) + p2 * t * u + p3 * (1 - t) * u;
       Rx = (1 - u) * (p1 - p0) + u * (p2 - p3);
       Ry = (1 - t) * (p3 - p0) + t * (p2 - p1);
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        const float* Dq = D0 + q * dstride;
-        Dv[q] = Dq[k0] * (1 - t) * (1 - u) + Dq[k1] * t * (1 - u) + Dq[k2] * t * u + Dq[k3] * (1 - t) * u;
+        const V* Dq = D0 + q * dstride;
+        Dv[q] = to_d(Dq[k0]) * (1 - t) * (1 - u) + to_d(Dq[k1]) * t * (1 - u) + to_d(Dq[k2]) * t * u +
+                to_d(Dq[k3]) * (1 - t) * u;
       }
     }
     const double a = m * R;
@@ -262,9 +283,24 @@ void window_sums(const float* img, int nx, int ny, const int* offx, const int* o
   GISSPA_LAUNCH_CHECK();
 }
 
+void round_templates(const float* prep, long long n, int precision, void* out, cudaStream_t s) {
+  if (precision == GISSPA_SPEC_FP16)
+    round_kernel<__half><<<ceil_div(n, 256), 256, 0, s>>>(prep, n, static_cast<__half*>(out));
+  else
+    round_kernel<__nv_bfloat16><<<ceil_div(n, 256), 256, 0, s>>>(prep, n, static_cast<__nv_bfloat16*>(out));
+  GISSPA_LAUNCH_CHECK();
+}
+
 void score_grads(const GradArgs& g, const GradPick* picks, int n, float* out, cudaStream_t s) {
   if (n <= 0) return;
-  score_grad_kernel<<<n, kGT, 0, s>>>(g, picks, out);
+  if (g.precision == GISSPA_SPEC_FP16)
+    score_grad_kernel<__half><<<n, kGT, 0, s>>>(g, static_cast<const __half*>(g.prep_lp),
+                                                 static_cast<const __half*>(g.dprep_lp), picks, out);
+  else if (g.precision == GISSPA_SPEC_BF16)
+    score_grad_kernel<__nv_bfloat16><<<n, kGT, 0, s>>>(g, static_cast<const __nv_bfloat16*>(g.prep_lp),
+                                                        static_cast<const __nv_bfloat16*>(g.dprep_lp), picks, out);
+  else
+    score_grad_kernel<float><<<n, kGT, 0, s>>>(g, g.prep, g.dprep, picks, out);
   GISSPA_LAUNCH_CHECK();
 }
 

@@ -15,6 +15,11 @@ struct GradPick {
 struct GradArgs {
   const float* prep;       // [nt][L][L] prepared templates (real space) at the CTF evaluated
   const float* dprep;      // [3][nt][L][L] d prep / d(dfu, dfv, dfang)
+  // The same two arrays stored in the handle's template precision (GISSPA_SPEC_FP16 / BF16:
+  // 2-byte values read in place of prep / dprep); precision GISSPA_SPEC_FP32 reads the above.
+  const void* prep_lp;
+  const void* dprep_lp;
+  int precision;
   const float* img;        // [ny][nx] preprocessed micrograph
   int nx, ny;
   const int* offx;
@@ -33,6 +38,8 @@ void ctf_dweight(float* dtab, int l, const DevParams& p, cudaStream_t s);
 void scale_by_table(const float2* F, const float* tab, const double* m, int nt, int l, float2* out, cudaStream_t s);
 void window_sums(const float* img, int nx, int ny, const int* offx, const int* offy, int bx, int nwin, int l,
                  const double* win_m, double* out, cudaStream_t s);
+// prep (n values) rounded to the template precision (1: FP16, 2: BF16) into out
+void round_templates(const float* prep, long long n, int precision, void* out, cudaStream_t s);
 // out: n x 7 floats (z, dz/d(dx, dy, theta, dfu, dfv, dfang))
 void score_grads(const GradArgs& g, const GradPick* picks, int n, float* out, cudaStream_t s);
 

@@ -164,9 +164,8 @@ __global__ void gen_nonorm_kernel(const float2* __restrict__ X, CorrArgs a, int 
   atomicAdd(a.nn_sum + 2 * qq + 1, b2);
   const float vb = key_float((uint32_t)(best >> 32));
   if (vb > 0.f) {
-    const int tb = brev8(255 - (unsigned)(best & 0xffu));
     const unsigned long long g =
-        ((unsigned long long)float_key(vb) << 32) | ((unsigned long long)(0xFFFFFu - chunk) << 8) | tb;
+        ((unsigned long long)float_key(vb) << 32) | ((unsigned long long)(0xFFFFFu - chunk) << 8) | (best & 0xffu);
     atomicMax(a.nn_key + qq, g);
   }
 }
@@ -404,9 +403,8 @@ __global__ void __launch_bounds__(256) gen_rows_kernel(const float2* __restrict_
           const float vb = key_float((uint32_t)(best >> 32));
           if (vb > 0.f) {
             const int chunk = Y0 * L / 256 + i;
-            const int tb = brev8(255 - (unsigned)(best & 0xffu));
-            atomicMax(a.nn_key + qq,
-                      ((unsigned long long)float_key(vb) << 32) | ((unsigned long long)(0xFFFFFu - chunk) << 8) | tb);
+            atomicMax(a.nn_key + qq, ((unsigned long long)float_key(vb) << 32) |
+                                         ((unsigned long long)(0xFFFFFu - chunk) << 8) | (best & 0xffu));
           }
         }
       } else if constexpr (EPI == EPI_MAP) {
@@ -477,7 +475,7 @@ bool generic_fused(int L, int epi) {
   return rb > 0 && gen_rows_smem(L, rb, epi, 1) <= kGenSmemMax && (size_t)2 * sizeof(float2) * L <= kGenSmemMax;
 }
 
-bool correlate_fast(int L) { return L == 256 || L == 512 || L == 1024; }
+bool correlate_fast(int L) { return L == 256 || L == 320 || L == 512 || L == 1024; }
 
 size_t generic_z_elems(int L, int P) { return (size_t)P * (L / 2 + 1) * L; }
 size_t generic_x_elems(int L, int P, int epi) { return generic_fused(L, epi) ? 0 : (size_t)P * L * L; }

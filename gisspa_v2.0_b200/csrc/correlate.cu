@@ -28,8 +28,29 @@ struct TeamSync {
 template <int L>
 struct PassA;
 template <> struct PassA<256> { static constexpr int TT = 16, NC = 16; };
+template <> struct PassA<320> { static constexpr int TT = 16, NC = 16; };
 template <> struct PassA<512> { static constexpr int TT = 16, NC = 16; };
 template <> struct PassA<1024> { static constexpr int TT = 32, NC = 8; };
+
+// The column transform of pass A: two Stockham stages (one exchange) for the powers of two,
+// three (20 x 4 x 4, two exchanges) for 320, whose 20 points per lane allow no two-stage plan
+// with every lane busy.
+template <int L, int TT>
+struct ColXform {
+  __device__ __forceinline__ static int in_index(int tid, int e) { return fft2_in_index<L, TT>(tid, e); }
+  __device__ __forceinline__ static int out_index(int tid, int e) { return fft2_out_index<L, TT>(tid, e); }
+  __device__ __forceinline__ static void run(float2* v, float2* sm, const float2* tw, int tid) {
+    fft2s<L, TT, +1>(v, sm, TwGlobal{tw}, tid, WarpSync{});
+  }
+};
+template <>
+struct ColXform<320, 16> {
+  __device__ __forceinline__ static int in_index(int tid, int e) { return fft3_in_index<320, 16>(tid, e); }
+  __device__ __forceinline__ static int out_index(int tid, int e) { return fft3_out_index<320, 16>(tid, e); }
+  __device__ __forceinline__ static void run(float2* v, float2* sm, const float2* tw, int tid) {
+    fft3<320, 16, +1>(v, sm, TwGlobal{tw}, tid, WarpSync{});
+  }
+};
 
 // Pass A: one team of TT threads per column slot, NC slots per CTA, one pair per blockIdx.y.
 // Each column is a two-stage Stockham transform (32 x 16 points at L = 512) with E = L / TT
@@ -45,6 +66,7 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC, 2)
     pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
                   int b0, int n0, int D, const float2* __restrict__ twL, int chained) {
   constexpr int TT = PassA<L>::TT, NC = PassA<L>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
+  using CX = ColXform<L, TT>;
   constexpr int SH = NC >= 16 ? 0 : NC == 8 ? 1 : 2;
   static_assert(NC == 4 || NC == 8 || NC == 16, "swizzle assumes 4, 8 or 16 slots per CTA");
   static_assert(TT <= 32 && 32 % TT == 0, "a team lies inside one warp");
@@ -62,7 +84,7 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC, 2)
     // columns kx = 0 and kx = L/2 have real inverse transforms: pack them as a + i b
 #pragma unroll
     for (int i = 0; i < E; ++i) {
-      const int ky = fft2_in_index<L, TT>(tid, i);
+      const int ky = CX::in_index(tid, i);
       const float2 a = cmulc(Ib[ky], SPEC::load(Tn + ky));
       const float2 b = cmulc(Ib[(size_t)NZ * L + ky], SPEC::load(Tn + (size_t)NZ * L + ky));
       v[i] = make_float2(a.x - b.y, a.y + b.x);
@@ -72,15 +94,15 @@ __global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC, 2)
     const typename SPEC::T* Tc = Tn + (size_t)c * L;
 #pragma unroll
     for (int i = 0; i < E; ++i) {
-      const int ky = fft2_in_index<L, TT>(tid, i);
+      const int ky = CX::in_index(tid, i);
       v[i] = cmulc(__ldg(Ic + ky), SPEC::load(Tc + ky));
     }
   }
-  fft2s<L, TT, +1>(v, smem + team * L, TwGlobal{twL}, tid, WarpSync{});
+  CX::run(v, smem + team * L, twL, tid);
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < E; ++i) {
-    const int y = fft2_out_index<L, TT>(tid, i);
+    const int y = CX::out_index(tid, i);
     smem[y * NC + (team ^ ((y >> SH) & (NC - 1)))] = v[i];
   }
   __syncthreads();
@@ -121,6 +143,101 @@ __device__ __forceinline__ bool team_any(bool pred) {
   }
 }
 
+// The row transform of pass B: the Hermitian half row (NZ + 1 values, the kx = 0 and kx = L/2
+// terms packed in slot 0) becomes L real values through a length-NZ complex inverse transform
+// of Z[k] = E[k] + i W_L^-k O[k] (E, O: the even / odd parts of the half row) and lane output j
+// = (x[2j], x[2j + 1]).  EIN inputs and EOUT outputs per lane; the row's shared-memory slice is
+// the exchange buffer once every lane of the team has read its inputs.
+template <int NZ>
+__device__ __forceinline__ float2 row_unpack(const float2* row, const float2* tw_l, int k) {
+  float2 xk, xm;
+  if (k == 0) {
+    const float2 q = row[0];
+    xk = make_float2(q.x, 0.f);
+    xm = make_float2(q.y, 0.f);
+  } else {
+    xk = row[k];
+    xm = row[NZ - k];
+  }
+  const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
+  const float2 od = make_float2(xk.x - xm.x, xk.y + xm.y);
+  float2 w = tw_l[k];
+  w.y = -w.y;
+  const float2 o = cmul(w, od);
+  return make_float2(ev.x - o.y, ev.y + o.x);
+}
+template <int L, int TEAM>
+struct RowXform {
+  static constexpr int NZ = L / 2, EIN = NZ / TEAM, EOUT = NZ / TEAM, EBUF = EIN;
+  __device__ __forceinline__ static int out_index(int lt, int i) { return fft3_out_index<NZ, TEAM>(lt, i); }
+  template <typename Sync>
+  __device__ __forceinline__ static void run(float2* v, float2* row, const float2* tw_nz, const float2* tw_l, int lt,
+                                             Sync tsync) {
+#pragma unroll
+    for (int i = 0; i < EIN; ++i) v[i] = row_unpack<NZ>(row, tw_l, fft3_in_index<NZ, TEAM>(lt, i));
+    tsync();  // every lane of the team has read the row before the transform overwrites it
+    fft3<NZ, TEAM, +1>(v, row, TwShared{tw_nz}, lt, tsync);
+  }
+};
+// Window 320: the 160-point row transform on 16 lanes as two Stockham stages, radix 16 then
+// radix 10.  Stage 1 has 10 butterflies (lanes 0-9, 16 inputs x[j + 10 m] each); stage 2 has
+// 16 (every lane, 10 inputs x[j + 16 m] with twiddles W_160^(j m)) and leaves lane j the outputs
+// X[j + 16 r], r < 10: 20 pixels per lane, so the per-pixel accumulators of the epilogues stay
+// in registers.  The exchange goes through the row's slice with the 16-slot XOR swizzle.
+template <>
+struct RowXform<320, 16> {
+  static constexpr int NZ = 160, EIN = 16, EOUT = 10, EBUF = 16;
+  __device__ __forceinline__ static int out_index(int lt, int i) { return lt + 16 * i; }
+  template <typename Sync>
+  __device__ __forceinline__ static void run(float2* v, float2* row, const float2* tw_nz, const float2* tw_l, int lt,
+                                             Sync tsync) {
+    if (lt < 10) {
+#pragma unroll
+      for (int m = 0; m < EIN; ++m) v[m] = row_unpack<NZ>(row, tw_l, lt + 10 * m);
+    }
+    tsync();
+    if (lt < 10) {
+      Dft<16, +1>::run(v);
+#pragma unroll
+      for (int r = 0; r < 16; ++r) row[fft_swz<4>(lt * 16 + r)] = v[r];
+    }
+    tsync();
+#pragma unroll
+    for (int m = 0; m < 10; ++m) v[m] = row[fft_swz<4>(lt + 16 * m)];
+    float2 w[10];
+    tw_powers<10>(table_tw<+1>(TwShared{tw_nz}, lt), w);
+#pragma unroll
+    for (int m = 1; m < 10; ++m) v[m] = cmul(v[m], w[m]);
+    Dft<10, +1>::run(v);
+  }
+};
+
+// A chunk pick: the chunk's best key (z, 255 - brev8(position in the chunk)) at or above the
+// threshold whose pixel's centre passes the border test becomes a candidate (norm.cu:583-597).
+template <int L>
+__device__ __forceinline__ void emit_chunk(const CorrArgs& a, unsigned long long key, int chunk, int win, int templ,
+                                           int angle) {
+  const float zb = key_float((uint32_t)(key >> 32));
+  if (!(zb >= a.thresh)) return;
+  const int t = brev8(255 - (unsigned)(key & 0xffu));
+  const int id = chunk * 256 + t;
+  const int px = id % L, py = id / L;
+  const int cx = a.offx[win % a.bx] + px, cy = a.offy[win / a.bx] + py;
+  if (!(cx >= a.dmin && cx < a.nx - a.dmin && cy >= a.dmin && cy < a.ny - a.dmin)) return;
+  const unsigned slot = atomicAdd(a.cand_count, 1u);
+  if (slot >= a.cand_cap) return;
+  Cand cd;
+  cd.score = zb;
+  cd.x = px;
+  cd.y = py;
+  cd.window = win;
+  cd.templ = templ;
+  cd.angle = angle;
+  cd.chunk = chunk;
+  cd.pad = 0;
+  a.cand[slot] = cd;
+}
+
 // Pass B: a team (TEAM lanes) per output row; RB rows per CTA, one window per blockIdx.y,
 // looping over the launch's D templates.  The RB rows of each template are one
 // contiguous block of Q: one bulk asynchronous copy per template into a
@@ -130,7 +247,8 @@ __device__ __forceinline__ bool team_any(bool pred) {
 template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB)
     pass_b_kernel(CorrArgs a, const float2* __restrict__ twL, const float2* __restrict__ twNZ) {
-  constexpr int NZ = L / 2, E = NZ / TEAM, NTEAM = NW * 32 / TEAM, RPT = RB / NTEAM;
+  using RX = RowXform<L, TEAM>;
+  constexpr int NZ = L / 2, E = RX::EOUT, NTEAM = NW * 32 / TEAM, RPT = RB / NTEAM;
   static_assert(TEAM <= 32 || (TEAM % 32 == 0 && NTEAM <= 15), "a wide team is whole warps with its own barrier");
   constexpr unsigned kStageBytes = RB * NZ * sizeof(float2);
   static_assert(RB % NTEAM == 0, "rows must split evenly over teams");
@@ -146,11 +264,21 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   const int team = threadIdx.x / TEAM, lt = threadIdx.x - team * TEAM;
   const int e = blockIdx.y, y0 = blockIdx.x * RB, win = a.b0 + e;
   const int angle = a.angle_state ? a.angle_state->index : a.angle;
+  // L = 320: the CTA's output rows (L/2 + y0 ...) hold whole chunks (RB a multiple of 4 that
+  // divides L/2: 4 rows = 5 chunks, and the rows never wrap inside one CTA); their maxima are
+  // gathered per template in chunk_part
+  static_assert(L % 256 == 0 || (L == 320 && RB % 4 == 0 && (L / 2) % RB == 0), "chunks must not leave the CTA");
+  constexpr int kChunks = (L % 256 == 0 || EPI != EPI_CHUNK) ? 1 : RB * L / 256;
+  __shared__ unsigned long long chunk_part[kChunks];
+  const int cbase = (((y0 + L / 2) % L) * L) >> 8;
+  if (L % 256 != 0 && EPI == EPI_CHUNK)
+    for (int q = threadIdx.x; q < kChunks; q += NW * 32) chunk_part[q] = 0ull;
   // The correlation is the raw transform times 1/L^2, a power of two: scaling by it commutes
   // exactly with float rounding (no overflow or underflow at these magnitudes), so the sums,
   // the running maxima and the z-scores work on raw values and apply it once, bit for bit
   // as if every value had been scaled first.
-  static_assert((L & (L - 1)) == 0, "window size a power of two");
+  // (For L = 320 the factor is not a power of two; applying it once instead of to every value
+  // then changes the results by FP32 rounding only.)
   const float inv = 1.0f / (float)(L * L);
   const size_t wbase = (size_t)win * L * L;
   if (threadIdx.x == 0) {
@@ -172,7 +300,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   // per-lane pixel coordinates: element i, half h -> (out_y of row s, out_x)
   int ox[E];
 #pragma unroll
-  for (int i = 0; i < E; ++i) ox[i] = (2 * fft3_out_index<NZ, TEAM>(lt, i) + L / 2) & (L - 1);
+  for (int i = 0; i < E; ++i) ox[i] = (2 * RX::out_index(lt, i) + L / 2) % L;
 
   float acc1[RPT][E][2], acc2[RPT][E][2];
   float best[(EPI == EPI_TOPK) ? RPT : 1][E][2];
@@ -196,7 +324,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   if constexpr (EPI == EPI_CHUNK) {
 #pragma unroll
     for (int s = 0; s < RPT; ++s) {
-      const int oy = (y0 + team + NTEAM * s + L / 2) & (L - 1);
+      const int oy = (y0 + team + NTEAM * s + L / 2) % L;
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const float4 m = *reinterpret_cast<const float4*>(a.musig + wbase + (size_t)oy * L + ox[i]);
@@ -229,31 +357,11 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
     for (int s = 0; s < RPT; ++s) {
       const int r = team + NTEAM * s;
-      const int oy = (y0 + r + L / 2) & (L - 1);
+      const int oy = (y0 + r + L / 2) % L;
       float2* row = stg + r * NZ;
-      float2 v[E];
-#pragma unroll
-      for (int i = 0; i < E; ++i) {
-        const int k = fft3_in_index<NZ, TEAM>(lt, i);
-        float2 xk, xm;
-        if (k == 0) {
-          const float2 q = row[0];
-          xk = make_float2(q.x, 0.f);
-          xm = make_float2(q.y, 0.f);
-        } else {
-          xk = row[k];
-          xm = row[NZ - k];
-        }
-        const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
-        const float2 od = make_float2(xk.x - xm.x, xk.y + xm.y);
-        float2 w = tw_l[k];
-        w.y = -w.y;
-        const float2 o = cmul(w, od);
-        v[i] = make_float2(ev.x - o.y, ev.y + o.x);
-      }
+      float2 v[RX::EBUF];
       const TeamSync<TEAM> tsync{1 + team};
-      tsync();  // every lane of the team has read the row before the transform overwrites it
-      fft3<NZ, TEAM, +1>(v, row, TwShared{tw_nz}, lt, tsync);
+      RX::run(v, row, tw_nz, tw_l, lt, tsync);
 
       if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll
@@ -271,7 +379,11 @@ __global__ void __launch_bounds__(NW * 32, MINB)
             }
           }
       } else if constexpr (EPI == EPI_CHUNK) {
-        constexpr int CPR = L >= 256 ? L / 256 : 1;  // chunks per row
+        // chunks (256 consecutive pixels of the window's linear index) touched by one row: whole
+        // chunks for L a multiple of 256; at L = 320 a row starts 0, 64, 128 or 192 pixels into
+        // a chunk and always touches two, each shared with a neighbouring row
+        constexpr int CPR = L % 256 == 0 ? L / 256 : 2;
+        const int c0 = (oy * L) >> 8;
         // a team wider than a warp (two warps per row) meets in shared memory: the warps'
         // votes and chunk maxima, behind the team's barrier (the next writes come after the
         // next row's barriers)
@@ -309,7 +421,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
               for (int h = 0; h < 2; ++h) {
                 const int x = ox[i] + h;
-                if ((x >> 8) != ch) continue;
+                if (((oy * L + x) >> 8) - c0 != ch) continue;
                 const int t = (oy * L + x) & 255;
                 const unsigned long long k2 =
                     ((unsigned long long)float_key(z[i][h]) << 32) | (unsigned)(255 - brev8(t));
@@ -317,49 +429,34 @@ __global__ void __launch_bounds__(NW * 32, MINB)
               }
             keys[ch] = team_max_u64<(TEAM > 32 ? 32 : TEAM)>(key);
           }
-          if constexpr (TEAM > 32) {
-            if ((threadIdx.x & 31) == 0)
-#pragma unroll
-              for (int ch = 0; ch < CPR; ++ch) chunk_key[team][wid][ch] = keys[ch];
-            tsync();
+          if constexpr (L % 256 != 0) {
+            // the row's part of each chunk meets the other row's in shared memory; the chunks
+            // are complete once every team has done this template (see after the row loop)
             if (lt == 0)
 #pragma unroll
-              for (int ch = 0; ch < CPR; ++ch)
+              for (int ch = 0; ch < CPR; ++ch) atomicMax(&chunk_part[c0 + ch - cbase], keys[ch]);
+          } else {
+            if constexpr (TEAM > 32) {
+              if ((threadIdx.x & 31) == 0)
 #pragma unroll
-                for (int w = 1; w < WT; ++w) keys[ch] = keys[ch] > chunk_key[team][w][ch] ? keys[ch] : chunk_key[team][w][ch];
-          }
+                for (int ch = 0; ch < CPR; ++ch) chunk_key[team][wid][ch] = keys[ch];
+              tsync();
+              if (lt == 0)
 #pragma unroll
-          for (int ch = 0; ch < CPR; ++ch) {
-            const unsigned long long key = keys[ch];
-            if (lt == 0) {
-              const float zb = key_float((uint32_t)(key >> 32));
-              if (zb >= a.thresh) {
-                const int t = brev8(255 - (unsigned)(key & 0xffu));
-                const int id = ((oy * L + ch * 256) & ~255) + t;
-                const int px = id % L, py = id / L;
-                const int cx = a.offx[win % a.bx] + px, cy = a.offy[win / a.bx] + py;
-                if (cx >= a.dmin && cx < a.nx - a.dmin && cy >= a.dmin && cy < a.ny - a.dmin) {
-                  const unsigned slot = atomicAdd(a.cand_count, 1u);
-                  if (slot < a.cand_cap) {
-                    Cand cd;
-                    cd.score = zb;
-                    cd.x = px;
-                    cd.y = py;
-                    cd.window = win;
-                    cd.templ = a.n0 + d;
-                    cd.angle = angle;
-                    cd.chunk = id >> 8;
-                    cd.pad = 0;
-                    a.cand[slot] = cd;
-                  }
-                }
-              }
+                for (int ch = 0; ch < CPR; ++ch)
+#pragma unroll
+                  for (int w = 1; w < WT; ++w)
+                    keys[ch] = keys[ch] > chunk_key[team][w][ch] ? keys[ch] : chunk_key[team][w][ch];
             }
+            if (lt == 0)
+#pragma unroll
+              for (int ch = 0; ch < CPR; ++ch) emit_chunk<L>(a, keys[ch], c0 + ch, win, a.n0 + d, angle);
           }
         }
       } else if constexpr (EPI == EPI_NONORM) {
         static_assert(TEAM <= 32, "peak and sums reduce within a warp");
-        constexpr int CPR = L >= 256 ? L / 256 : 1;
+        constexpr int CPR = L % 256 == 0 ? L / 256 : 2;
+        const int c0 = (oy * L) >> 8;
         // get_peak_and_SUM (kernels.cu:725-763): sums over every pixel, max with the
         // border (closer than diameter/4 to the window edge) forced to 0
 #pragma unroll
@@ -375,7 +472,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
               const int x = ox[i] + h;
-              if ((x >> 8) != ch) continue;
+              if (((oy * L + x) >> 8) - c0 != ch) continue;
               float val = h ? v[i].y : v[i].x;
               if (x < a.border || x > L - a.border || oy < a.border || oy > L - a.border) val = 0.f;
               const int t = (oy * L + x) & 255;
@@ -387,10 +484,11 @@ __global__ void __launch_bounds__(NW * 32, MINB)
           if (lt == 0) {
             const float vb = key_float((uint32_t)(key >> 32));
             if (vb > 0.f) {
-              const int t = brev8(255 - (unsigned)(key & 0xffu));
-              const int chunk = ((oy * L + ch * 256) >> 8);
-              const unsigned long long g =
-                  ((unsigned long long)float_key(vb) << 32) | ((unsigned long long)(0xFFFFFu - chunk) << 8) | t;
+              // largest value, then the lowest chunk, then the reference's in-chunk order (the
+              // byte 255 - brev8(t)): parts of one chunk from two rows combine correctly
+              const int chunk = c0 + ch;
+              const unsigned long long g = ((unsigned long long)float_key(vb) << 32) |
+                                           ((unsigned long long)(0xFFFFFu - chunk) << 8) | (key & 0xffu);
               atomicMax(a.nn_key + (size_t)win * a.nt_total + a.n0 + d, g);
             }
           }
@@ -400,6 +498,14 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
         for (int i = 0; i < E; ++i)
           *reinterpret_cast<float2*>(out + ox[i]) = make_float2(v[i].x * inv, v[i].y * inv);
+      }
+    }
+    if constexpr (EPI == EPI_CHUNK && L % 256 != 0) {
+      __syncthreads();  // every row part of this template's chunks is in
+      for (int q = threadIdx.x; q < kChunks; q += NW * 32) {
+        const unsigned long long key = chunk_part[q];
+        chunk_part[q] = 0ull;
+        if (key) emit_chunk<L>(a, key, cbase + q, win, a.n0 + d, angle);
       }
     }
     if constexpr (EPI == EPI_NONORM) {
@@ -421,7 +527,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll
     for (int s = 0; s < RPT; ++s) {
-      const int oy = (y0 + team + NTEAM * s + L / 2) & (L - 1);
+      const int oy = (y0 + team + NTEAM * s + L / 2) % L;
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         const size_t pix = wbase + (size_t)oy * L + ox[i];
@@ -497,6 +603,11 @@ template <> struct PassB<512, 0> { static constexpr int TEAM = 32, RB = 16, NW =
 template <> struct PassB<512, 1> { static constexpr int TEAM = 32, RB = 8, NW = 8, MINB = 2; };
 template <> struct PassB<512, 2> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 8; };
 template <> struct PassB<512, 3> { static constexpr int TEAM = 32, RB = 1, NW = 1, MINB = 16; };
+// window 320: 16-lane rows (the 16 x 10 row plan), RB a multiple of 4 dividing 160 so that the
+// chunk picks stay inside the CTA
+template <> struct PassB<320, 0> { static constexpr int TEAM = 16, RB = 16, NW = 8, MINB = 1; };
+template <> struct PassB<320, 1> { static constexpr int TEAM = 16, RB = 8, NW = 4, MINB = 2; };
+template <> struct PassB<320, 2> { static constexpr int TEAM = 16, RB = 4, NW = 2, MINB = 4; };
 template <> struct PassB<1024, 0> { static constexpr int TEAM = 32, RB = 8, NW = 8, MINB = 1; };
 template <> struct PassB<1024, 1> { static constexpr int TEAM = 32, RB = 2, NW = 2, MINB = 2; };
 // the same, capped at 168 registers (6 CTAs per SM): no spills for the sum and chunk epilogues
@@ -548,6 +659,12 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
       case 3: launch_b<L, 3>(cl, args, twL, twNZ, s); break;
       default: launch_b<L, 0>(cl, args, twL, twNZ, s); break;
     }
+  } else if constexpr (L == 320) {
+    switch (cl.variant) {
+      case 1: launch_b<L, 1>(cl, args, twL, twNZ, s); break;
+      case 2: launch_b<L, 2>(cl, args, twL, twNZ, s); break;
+      default: launch_b<L, 0>(cl, args, twL, twNZ, s); break;
+    }
   } else if constexpr (L == 1024) {
     switch (cl.variant) {
       case 1: launch_b<L, 1>(cl, args, twL, twNZ, s); break;
@@ -570,7 +687,7 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
 
 bool correlate_supported(int L) { return L == 256 || L == 512 || L == 1024; }
 
-int correlate_variants(int L) { return L == 512 ? 4 : L == 1024 ? 5 : 2; }
+int correlate_variants(int L) { return L == 512 ? 4 : L == 1024 ? 5 : L == 320 ? 3 : 2; }
 
 bool correlate_variant_ok(int L, int variant, int epi) {
   if (variant < 0 || variant >= correlate_variants(L)) return false;
@@ -582,6 +699,7 @@ int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {
   switch (cl.L) {
     case 256: return launch_pair<256>(cl, I, T, Q, args, twL, twNZ, s, ev);
+    case 320: return launch_pair<320>(cl, I, T, Q, args, twL, twNZ, s, ev);
     case 512: return launch_pair<512>(cl, I, T, Q, args, twL, twNZ, s, ev);
     case 1024: return launch_pair<1024>(cl, I, T, Q, args, twL, twNZ, s, ev);
     default: throw CudaError{cudaErrorInvalidValue, "window size without correlation kernels"};

@@ -38,6 +38,39 @@ __host__ __device__ constexpr double cos32(int k) {
 }
 __host__ __device__ constexpr double sin32(int k) { return cos32(k - 8); }
 
+// cos(2 pi k / 20) and sin(2 pi k / 20) for any integer k, from cos(j pi / 10), j = 0..5
+// (cos 18 deg = sqrt(10 + 2 sqrt 5) / 4, cos 36 deg = (1 + sqrt 5) / 4, cos 54 deg =
+// sqrt(10 - 2 sqrt 5) / 4, cos 72 deg = (sqrt 5 - 1) / 4).
+__host__ __device__ constexpr double cos20(int k) {
+  constexpr double c[6] = {1.0,
+                           0.95105651629515357212,
+                           0.80901699437494742410,
+                           0.58778525229247312917,
+                           0.30901699437494742410,
+                           0.0};
+  k %= 20;
+  if (k < 0) k += 20;
+  return k <= 5 ? c[k] : k <= 10 ? -c[10 - k] : k <= 15 ? -c[k - 10] : c[20 - k];
+}
+__host__ __device__ constexpr double sin20(int k) { return cos20(k - 5); }
+
+// cos and sin of 2 pi K / R for a radix R dividing 32 or 20.
+template <int R>
+__host__ __device__ constexpr double root_cos(int k) {
+  static_assert(32 % R == 0 || 20 % R == 0, "roots of unity for radices dividing 32 or 20");
+  if constexpr (32 % R == 0)
+    return cos32((32 / R) * k);
+  else
+    return cos20((20 / R) * k);
+}
+template <int R>
+__host__ __device__ constexpr double root_sin(int k) {
+  if constexpr (32 % R == 0)
+    return sin32((32 / R) * k);
+  else
+    return sin20((20 / R) * k);
+}
+
 // Multiply v by W_R^K = exp(SIGN * 2 pi i K / R) (R dividing 32) with exact special cases.
 template <int R, int K, int SIGN>
 __device__ __forceinline__ float2 mul_wr(float2 v) {
@@ -57,12 +90,78 @@ __device__ __forceinline__ float2 mul_wr(float2 v) {
     constexpr float h = 0.70710678118654752440f;
     return make_float2(h * (-v.x - SIGN * v.y), h * (-v.y + SIGN * v.x));
   } else {
-    static_assert(32 % R == 0, "radix must divide 32");
-    constexpr int k32 = (32 / R) * KK;  // in units of 2 pi / 32
-    constexpr float c = (float)cos32(k32), s = (float)(SIGN * sin32(k32));
+    constexpr float c = (float)root_cos<R>(KK), s = (float)(SIGN * root_sin<R>(KK));
     return make_float2(v.x * c - v.y * s, v.x * s + v.y * c);
   }
 }
+
+template <int R, int SIGN>
+struct Dft;
+
+// 5-point DFT: X_k = sum_n x_n e^(SIGN 2 pi i n k / 5) from the symmetric pairs
+// t1 = x1 + x4, t2 = x2 + x3, t3 = x1 - x4, t4 = x2 - x3:
+//   X1, X4 = x0 + c1 t1 + c2 t2 +- SIGN i (s1 t3 + s2 t4)
+//   X2, X3 = x0 + c2 t1 + c1 t2 +- SIGN i (s2 t3 - s1 t4)
+// with c_k = cos(2 pi k / 5), s_k = sin(2 pi k / 5).
+template <int SIGN>
+struct Dft<5, SIGN> {
+  __device__ __forceinline__ static void run(float2* a) {
+    constexpr float c1 = (float)cos20(4), c2 = (float)cos20(8), s1 = (float)sin20(4), s2 = (float)sin20(8);
+    const float2 t1 = cadd(a[1], a[4]), t2 = cadd(a[2], a[3]), t3 = csub(a[1], a[4]), t4 = csub(a[2], a[3]);
+    const float2 x0 = a[0];
+    const float2 p1 = make_float2(x0.x + c1 * t1.x + c2 * t2.x, x0.y + c1 * t1.y + c2 * t2.y);
+    const float2 p2 = make_float2(x0.x + c2 * t1.x + c1 * t2.x, x0.y + c2 * t1.y + c1 * t2.y);
+    // q = (s1 t3 + s2 t4), r = (s2 t3 - s1 t4); SIGN i q = SIGN (-q.y, q.x)
+    const float2 q = make_float2(s1 * t3.x + s2 * t4.x, s1 * t3.y + s2 * t4.y);
+    const float2 r = make_float2(s2 * t3.x - s1 * t4.x, s2 * t3.y - s1 * t4.y);
+    const float2 iq = make_float2(-SIGN * q.y, SIGN * q.x), ir = make_float2(-SIGN * r.y, SIGN * r.x);
+    a[0] = cadd(x0, cadd(t1, t2));
+    a[1] = cadd(p1, iq);
+    a[4] = csub(p1, iq);
+    a[2] = cadd(p2, ir);
+    a[3] = csub(p2, ir);
+  }
+};
+
+// Composite DFT of length A B (A a power of two, B = 5) in registers: n = B n1 + n2,
+// k = k1 + A k2:  X[k1 + A k2] = sum_n2 W_B^(n2 k2) W_AB^(n2 k1) (sum_n1 x[B n1 + n2] W_A^(n1 k1)).
+template <int A, int B, int SIGN>
+struct DftAB {
+  template <int N2, int K1>
+  __device__ __forceinline__ static void twiddle(float2 (&y)[B][A]) {
+    if constexpr (N2 < B) {
+      if constexpr (K1 < A) {
+        y[N2][K1] = mul_wr<A * B, N2 * K1, SIGN>(y[N2][K1]);
+        twiddle<N2, K1 + 1>(y);
+      } else {
+        twiddle<N2 + 1, 0>(y);
+      }
+    }
+  }
+  __device__ __forceinline__ static void run(float2* a) {
+    float2 y[B][A];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) y[n2][n1] = a[B * n1 + n2];
+      Dft<A, SIGN>::run(y[n2]);
+    }
+    twiddle<0, 0>(y);
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+      float2 z[B];
+#pragma unroll
+      for (int n2 = 0; n2 < B; ++n2) z[n2] = y[n2][k1];
+      Dft<B, SIGN>::run(z);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) a[k1 + A * k2] = z[k2];
+    }
+  }
+};
+template <int SIGN>
+struct Dft<10, SIGN> : DftAB<2, 5, SIGN> {};
+template <int SIGN>
+struct Dft<20, SIGN> : DftAB<4, 5, SIGN> {};
 
 // In-register DFT of length R (R in {1, 2, 4, 8, 16}), natural order in and out.
 template <int R, int SIGN>
@@ -149,7 +248,7 @@ __device__ __forceinline__ void stockham_stage(float2* v, float2* sm, const Tw& 
 #pragma unroll
   for (int q = 0; q < B; ++q) {
     const int j = tid + T * q;
-    const int k = j & (NS - 1);
+    const int k = j % NS;
     float2* a = v + q * R;
     if constexpr (NS > 1) {
       constexpr int step = N / (NS * R);
@@ -189,6 +288,8 @@ template <> struct Plan<512, 64> { static constexpr int R1 = 8, R2 = 8, R3 = 8, 
 template <> struct Plan<512, 32> { static constexpr int R1 = 16, R2 = 8, R3 = 4, S = 4; };
 template <> struct Plan<1024, 64> { static constexpr int R1 = 16, R2 = 16, R3 = 4, S = 4; };
 template <> struct Plan<128, 16> { static constexpr int R1 = 8, R2 = 4, R3 = 4, S = 3; };
+// window 320: columns of 320 points on 16 lanes (20 each, the first stage a 4 x 5 register DFT)
+template <> struct Plan<320, 16> { static constexpr int R1 = 20, R2 = 4, R3 = 4, S = 2; };
 
 // Full three-stage transform.  v: E inputs in first-stage order; on return v holds
 // the outputs in last-stage order.  sm: this team's buffer of N values; SYNC() must be a

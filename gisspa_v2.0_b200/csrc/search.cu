@@ -77,10 +77,6 @@ int validate_config(const gisspa_config& c, std::string& err) {
     err = "topk must be positive and exclusion_radius non-negative";
     return GISSPA_ERR_ARG;
   }
-  if (c.norm_type == 0 && c.pick_mode == GISSPA_PICK_TOPK) {
-    err = "top-K picking is defined for norm_type=1 only";
-    return GISSPA_ERR_UNSUPPORTED;
-  }
   if (c.norm_type == 0 && c.tile_size <= 0) {
     err = "tile_size must be positive";
     return GISSPA_ERR_ARG;
@@ -817,6 +813,51 @@ void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_
 }
 
 // norm_type = 0 (SearchNoNorm, nonorm.cu): 720^2 tiles, rotate the windows, per-template best.
+// One norm_type=0 peak: the best pixel of one (tile, angle, window, template) map (the
+// reference's per-window peak, nonorm.cu:488-534), centre in micrograph coordinates.
+struct NonormCand {
+  double score;
+  float x, y;
+  int tile, angle, window;
+};
+
+// Per-template top-K with an exclusion radius over a template's norm_type=0 peaks (no
+// counterpart in the reference, which keeps one window per template, angle and tile): peaks in
+// descending score (ties in generation order: tile, angle, window), each taken unless it lies
+// within exclusion_radius of a peak already taken for the same template; at most topk.
+void nonorm_topk(std::vector<NonormCand>& cand, int n, const gisspa_config& cfg, const std::vector<float>& angles,
+                 std::vector<gisspa_pick>& out) {
+  std::stable_sort(cand.begin(), cand.end(),
+                   [](const NonormCand& u, const NonormCand& v) { return u.score > v.score; });
+  const double r2 = (double)cfg.exclusion_radius * cfg.exclusion_radius;
+  std::vector<const NonormCand*> taken;
+  for (const NonormCand& q : cand) {
+    if ((int)taken.size() >= cfg.topk) break;
+    bool ok = true;
+    for (const NonormCand* u : taken) {
+      const double dx = (double)q.x - u->x, dy = (double)q.y - u->y;
+      if (dx * dx + dy * dy <= r2) {
+        ok = false;
+        break;
+      }
+    }
+    if (!ok) continue;
+    gisspa_pick pk{};
+    pk.score = (float)q.score;
+    pk.x = q.x;
+    pk.y = q.y;
+    pk.angle = angles[q.angle];
+    pk.theta = angles[q.angle];
+    pk.template_id = n;
+    pk.window = q.window;
+    pk.tile = q.tile;
+    pk.angle_index = q.angle;
+    pk.chunk = (int)taken.size();
+    out.push_back(pk);
+    taken.push_back(&q);
+  }
+}
+
 void search_nonorm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_pick>& out) {
   gisspa_handle* h = c.h;
   const gisspa_config& cfg = h->cfg;
@@ -849,6 +890,10 @@ void search_nonorm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gissp
   std::vector<unsigned long long> hk((size_t)W * nt);
   std::vector<double> hsum((size_t)W * nt * 2);
   long long pairs = 0;
+  // top-K: every (tile, angle, window) peak of each template that passes the reference's
+  // centre test and the threshold, in that generation order
+  const bool topk = cfg.pick_mode == GISSPA_PICK_TOPK;
+  std::vector<std::vector<NonormCand>> cands(topk ? nt : 0);
   GISSPA_CUDA(cudaEventRecord(h->ev[1], c.s));
   for (size_t t = 0; t < tx.size(); ++t) {
     // LoadImage (nonorm.cu:157-165): the tile, inverted on request
@@ -917,10 +962,13 @@ void search_nonorm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gissp
             uint32_t bits = (hi & 0x80000000u) ? (hi & 0x7fffffffu) : ~hi;
             float pv;
             std::memcpy(&pv, &bits, 4);
+            // low word: (0xFFFFF - chunk) << 8 | (255 - brev8(position in the chunk))
             const unsigned lo = (unsigned)(k & 0xFFFFFFFFu);
             const int chunk = (int)(0xFFFFFu - (lo >> 8));
+            unsigned t = 255u - (lo & 0xFFu), tb = 0;
+            for (int bit = 0; bit < 8; ++bit) tb |= ((t >> bit) & 1u) << (7 - bit);
             peak = pv;
-            pos = (double)(chunk * 256 + (int)(lo & 0xFFu));
+            pos = (double)(chunk * 256 + (int)tb);
           }
           const double s1 = hsum[2 * ((size_t)b * nt + n)], s2 = hsum[2 * ((size_t)b * nt + n) + 1];
           const double rA = s1 - peak, rB = s2 - peak * peak, rC = (double)c.L2 - 1;
@@ -929,13 +977,21 @@ void search_nonorm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gissp
           const int cx = (int)pos % l, cy = (int)pos / l;
           const double centerx = i * (l - cfg.overlap) + (cx - l / 2) * ce + (cy - l / 2) * se + l / 2;
           const double centery = j * (l - cfg.overlap) + (cy - l / 2) * ce - (cx - l / 2) * se + l / 2;
-          if (bs[n] < (float)score && centerx >= 0 && centerx < ts && centery >= 0 && centery < ts) {
+          const bool valid = centerx >= 0 && centerx < ts && centery >= 0 && centery < ts;
+          if (topk) {
+            if (valid && (float)score >= cfg.threshold)
+              cands[n].push_back(NonormCand{score, (float)(tx[t] + centerx), (float)(ty[t] + centery), (int)t,
+                                            (int)a, b});
+            continue;
+          }
+          if (bs[n] < (float)score && valid) {
             bs[n] = (float)score;
             bxp[n] = (float)centerx;
             byp[n] = (float)centery;
           }
         }
       }
+      if (topk) continue;
       for (int n = 0; n < nt; ++n)  // OutputScore (nonorm.cu:539-557)
         if (bs[n] >= cfg.threshold) {
           gisspa_pick pk{};
@@ -954,6 +1010,9 @@ void search_nonorm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gissp
     }
   }
   GISSPA_CUDA(cudaEventRecord(h->ev[2], c.s));
+  if (topk) {
+    for (int n = 0; n < nt; ++n) nonorm_topk(cands[n], n, cfg, angles, out);
+  }
   GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
   h->st.pairs = pairs;
 }
@@ -1050,6 +1109,13 @@ void adjoint_prepare(gisspa_handle* h, const gisspa_ctf& ctf) {
   }
   window_sums(h->img_pre.as<float>(), h->last_nx, h->last_ny, h->offx.as<int>(), h->offy.as<int>(), h->last_bx,
               h->last_W, l, h->win_m.as<double>(), buf<double>(h->win_sum, h->last_W), c.s);
+  // the FP16 / BF16 template forms evaluate from templates stored at that precision
+  const int prec = h->cfg.spectrum_precision;
+  if (prec != GISSPA_SPEC_FP32) {
+    round_templates(h->prep_real.as<float>(), (long long)nt * c.L2, prec, buf<__half>(h->prep_lp, (size_t)nt * c.L2),
+                    c.s);
+    round_templates(dprep, 3LL * nt * c.L2, prec, buf<__half>(h->dprep_lp, 3 * (size_t)nt * c.L2), c.s);
+  }
 }
 
 void eval_grads(gisspa_handle* h, const std::vector<GradPick>& gp, std::vector<float>& out) {
@@ -1057,6 +1123,9 @@ void eval_grads(gisspa_handle* h, const std::vector<GradPick>& gp, std::vector<f
   GradArgs g{};
   g.prep = h->prep_real.as<float>();
   g.dprep = h->dprep.as<float>();
+  g.precision = h->cfg.spectrum_precision;
+  g.prep_lp = g.precision != GISSPA_SPEC_FP32 ? h->prep_lp.as<void>() : nullptr;
+  g.dprep_lp = g.precision != GISSPA_SPEC_FP32 ? h->dprep_lp.as<void>() : nullptr;
   g.img = h->img_pre.as<float>();
   g.nx = h->last_nx;
   g.ny = h->last_ny;

@@ -83,6 +83,7 @@ struct gisspa_handle {
   // adjoint: whitened template spectra before weighting, RMS factors, dW/dpsi tables,
   // d(prepared template)/dpsi, window RMS factors and sums
   gisspa::DevBuf tw_spec, tmpl_m, dtab, dprep, win_m, win_sum, grad_in, grad_out;
+  gisspa::DevBuf prep_lp, dprep_lp;  // adjoint templates at the FP16 / BF16 template precision
   bool keep_whitened = false;
   int last_nx = 0, last_ny = 0, last_W = 0, last_bx = 0;
   gisspa_ctf last_ctf{};

@@ -41,8 +41,12 @@ enum {
 enum {
   GISSPA_PICK_CHUNK = 0, /* reference picks: two sweeps, one pick per 256-pixel chunk
                             with z >= threshold (norm.cu:554-600) */
-  GISSPA_PICK_TOPK = 1   /* one sweep: per-pixel max z over templates x angles, then
-                            greedy top-K with an exclusion radius */
+  GISSPA_PICK_TOPK = 1   /* norm_type=1: one sweep, per-pixel max z over templates x angles,
+                            then greedy top-K with an exclusion radius.  norm_type=0: per
+                            template, every (tile, angle, window) peak with a valid centre and
+                            score >= threshold, then greedy top-K per template with the
+                            exclusion radius; centres in micrograph coordinates (tile
+                            offset added), pick.chunk = rank within the template */
 };
 
 /* ---- template-spectrum storage precision (FFT arithmetic is FP32 in all cases) ---- */
@@ -192,7 +196,9 @@ const char* gisspa_version(void);
  * reference).  mu and sigma are held at the pick pixel; the shift moves the template's
  * sampling (a Fourier shift on the periodic window), theta acts through the bilinear
  * rotation, and the CTF through the template-side |CTF| x SSNR weight (the micrograph's
- * preprocessing keeps the search's CTF). */
+ * preprocessing keeps the search's CTF).  With spectrum_precision FP16 or BF16 the prepared
+ * templates and their CTF derivatives are read as stored at that precision (half the bytes
+ * per pick); sums are FP64 in every form. */
 typedef struct gisspa_grad {
   float score;          /* z at the evaluated parameters */
   float d_dx, d_dy;     /* per pixel of shift of the pick centre */

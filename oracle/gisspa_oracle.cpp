@@ -639,9 +639,21 @@ int orc_rotated_spectrum(const gisspa_config* c, const gisspa_ctf* ctf, const do
 //  picks/cap/n_out: reference chunk picks (GISSPA_PICK_CHUNK) or top-K picks.
 //  stats_out (optional): W*l*l*2 doubles, per-window-pixel (mu, sigma).
 //  max_templates / max_angles (optional, > 0): restrict the search to a sample (timing only).
+//  margin_out (optional, cap doubles): for each pick, how far (in z) its outcome stands from the
+//    nearest alternative outcome; a pick whose margin is below twice a comparison tolerance may
+//    legitimately come out differently in FP32.  Chunk picks: best z of the chunk minus the
+//    next best pixel's.  Top-K picks: the smallest of (best z at the pixel minus the best z of
+//    any other (template, angle) there), (z minus the best z of the other candidate pixels within
+//    the exclusion radius that no earlier pick excluded) and, for the last pick, (z minus the
+//    next pick a larger K would take).
+//  near_out / near_margin (optional, chunk picks): chunks that gave no pick only because their
+//    best pixel's centre failed the border test although another pixel within 1 % of the best z
+//    passes it; each record is the pick that pixel would give (score = its z) and near_margin
+//    the z distance to the chunk's best.
 int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float* image, int nx, int ny,
                     const float* stack, int nt, int tw, int th, gisspa_pick* picks, size_t cap,
-                    size_t* n_out, double* stats_out, int max_templates, int max_angles) {
+                    size_t* n_out, double* stats_out, int max_templates, int max_angles, double* margin_out,
+                    gisspa_pick* near_out, double* near_margin, size_t near_cap, size_t* n_near) {
   int st = validate(cin, nx, ny, nt, tw, th);
   if (st) return st;
   gisspa_config c = *cin;
@@ -673,7 +685,12 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
   std::vector<double> S1((size_t)ws.W * L2, 0.0), S2((size_t)ws.W * L2, 0.0);
   std::vector<float> cmax;
   std::vector<int> carg;
-  if (topk) { cmax.assign((size_t)ws.W * L2, -INFINITY); carg.assign((size_t)ws.W * L2, -1); }
+  std::vector<double> cmax2;  // second-largest correlation at the pixel (margins only)
+  if (topk) {
+    cmax.assign((size_t)ws.W * L2, -INFINITY);
+    carg.assign((size_t)ws.W * L2, -1);
+    cmax2.assign((size_t)ws.W * L2, -INFINITY);
+  }
   std::vector<cd> T((size_t)nts * L2);
   for (int a = 0; a < n_angles_run; ++a) {
 #pragma omp parallel for schedule(dynamic)
@@ -696,9 +713,14 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
             double v = cc[k] / (double)L2;
             s1[k] += v;
             s2[k] += v * v;
-            if (topk && v > cmax[(size_t)b * L2 + k]) {
-              cmax[(size_t)b * L2 + k] = (float)v;
-              carg[(size_t)b * L2 + k] = a * nt + n;
+            if (topk) {
+              if (v > cmax[(size_t)b * L2 + k]) {
+                cmax2[(size_t)b * L2 + k] = std::max<double>(cmax2[(size_t)b * L2 + k], cmax[(size_t)b * L2 + k]);
+                cmax[(size_t)b * L2 + k] = (float)v;
+                carg[(size_t)b * L2 + k] = a * nt + n;
+              } else if (v > cmax2[(size_t)b * L2 + k]) {
+                cmax2[(size_t)b * L2 + k] = v;
+              }
             }
           }
         }
@@ -715,7 +737,8 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
   if (stats_out)
     for (size_t k = 0; k < mu.size(); ++k) { stats_out[2 * k] = mu[k]; stats_out[2 * k + 1] = sd[k]; }
 
-  std::vector<gisspa_pick> out;
+  std::vector<gisspa_pick> out, near;
+  std::vector<double> margins, near_m;
   if (!topk) {
     // sweep 2 (PickParticles norm.cu:554-600): z-score, 256-pixel chunk max, threshold,
     // centre inside [d, n-d)
@@ -724,7 +747,8 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
 #pragma omp parallel for schedule(dynamic)
       for (int n = 0; n < nts; ++n)
         rotated_template_spectrum(p, ws.prep.data() + (size_t)n * L2, l, angles[a], T.data() + (size_t)n * L2);
-      std::vector<std::vector<gisspa_pick>> per_b(ws.W);
+      std::vector<std::vector<gisspa_pick>> per_b(ws.W), near_b(ws.W);
+      std::vector<std::vector<double>> per_m(ws.W), near_mb(ws.W);
 #pragma omp parallel
       {
         std::vector<cd> buf;
@@ -739,27 +763,49 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
                          buf);
             const double* cc = ccs.data() + (n & 1) * L2;
             for (size_t ch = 0; ch < chunks; ++ch) {
-              double best = 0;
+              double best = 0, zs[256];
               unsigned blane = 0;
               for (unsigned t = 0; t < 256; ++t) {
                 size_t k = ch * 256 + t;
                 double s = sd[(size_t)b * L2 + k];
                 double z = s > 0 ? (cc[k] / (double)L2 - mu[(size_t)b * L2 + k]) / s : 0.0;
+                zs[t] = z;
                 if (t == 0 || chunk_better(z, t, best, blane)) { best = z; blane = t; }
               }
-              if (best >= p.thresh) {
-                size_t idx = ch * 256 + blane;
+              auto inside = [&](unsigned t) {
+                size_t idx = ch * 256 + t;
                 int cx = ws.offx[i] + (int)(idx % l), cy = ws.offy[j] + (int)(idx / l);
-                if (cx >= p.d_m && cx < nx - p.d_m && cy >= p.d_m && cy < ny - p.d_m) {
-                  gisspa_pick pk{};
-                  pk.score = (float)best;
-                  pk.x = (float)cx; pk.y = (float)cy;
-                  float cur_e = 360.0f - angles[a];
-                  if (cur_e >= 360.0f) cur_e -= 360.0f;
-                  pk.angle = cur_e;
-                  pk.theta = angles[a];
-                  pk.template_id = n; pk.window = b; pk.tile = 0; pk.angle_index = a; pk.chunk = (int)ch;
-                  per_b[b].push_back(pk);
+                return cx >= p.d_m && cx < nx - p.d_m && cy >= p.d_m && cy < ny - p.d_m;
+              };
+              auto make = [&](unsigned t, double z) {
+                size_t idx = ch * 256 + t;
+                gisspa_pick pk{};
+                pk.score = (float)z;
+                pk.x = (float)(ws.offx[i] + (int)(idx % l)); pk.y = (float)(ws.offy[j] + (int)(idx / l));
+                float cur_e = 360.0f - angles[a];
+                if (cur_e >= 360.0f) cur_e -= 360.0f;
+                pk.angle = cur_e;
+                pk.theta = angles[a];
+                pk.template_id = n; pk.window = b; pk.tile = 0; pk.angle_index = a; pk.chunk = (int)ch;
+                return pk;
+              };
+              if (best >= p.thresh && inside(blane)) {
+                per_b[b].push_back(make(blane, best));
+                if (margin_out) {
+                  double second = -INFINITY;
+                  for (unsigned t = 0; t < 256; ++t)
+                    if (t != blane) second = std::max(second, zs[t]);
+                  per_m[b].push_back(best - second);
+                }
+              } else if (near_out && best >= p.thresh - 0.01 * std::fabs(best)) {
+                // the best pixel's centre failed the border test: the best pixel that passes it
+                double bz = -INFINITY;
+                unsigned bt = 0;
+                for (unsigned t = 0; t < 256; ++t)
+                  if (t != blane && inside(t) && zs[t] > bz) { bz = zs[t]; bt = t; }
+                if (bz >= p.thresh - 0.01 * std::fabs(best) && best - bz <= 0.01 * std::fabs(best)) {
+                  near_b[b].push_back(make(bt, bz));
+                  near_mb[b].push_back(best - bz);
                 }
               }
             }
@@ -767,12 +813,21 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
         }
       }
       // output order: angle, window (j outer, i inner == b ascending), template, chunk
-      for (int b = 0; b < ws.W; ++b) out.insert(out.end(), per_b[b].begin(), per_b[b].end());
+      for (int b = 0; b < ws.W; ++b) {
+        out.insert(out.end(), per_b[b].begin(), per_b[b].end());
+        margins.insert(margins.end(), per_m[b].begin(), per_m[b].end());
+        near.insert(near.end(), near_b[b].begin(), near_b[b].end());
+        near_m.insert(near_m.end(), near_mb[b].begin(), near_mb[b].end());
+      }
     }
   } else {
     // one-sweep top-K: image map of max z over windows, then greedy exclusion
     std::vector<float> Z((size_t)nx * ny, -INFINITY);
     std::vector<int> Zarg((size_t)nx * ny, -1), Zwin((size_t)nx * ny, -1);
+    // per image pixel, for the margins: the best z of each window covering it with its
+    // (template, angle), and the best z of a second (template, angle) within any window
+    std::vector<double> Zalt;
+    if (margin_out) Zalt.assign((size_t)nx * ny, -INFINITY);
     for (int b = 0; b < ws.W; ++b) {
       int i = b % ws.bx, j = b / ws.bx;
       for (size_t k = 0; k < L2; ++k) {
@@ -782,9 +837,24 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
         int cx = ws.offx[i] + (int)(k % l), cy = ws.offy[j] + (int)(k / l);
         if (cx >= nx || cy >= ny) continue;
         size_t q = (size_t)cy * nx + cx;
+        if (margin_out && s > 0 && cmax2[(size_t)b * L2 + k] > -INFINITY)
+          Zalt[q] = std::max(Zalt[q], (cmax2[(size_t)b * L2 + k] - mu[(size_t)b * L2 + k]) / s);
         if ((float)z > Z[q]) { Z[q] = (float)z; Zarg[q] = carg[(size_t)b * L2 + k]; Zwin[q] = b; }
       }
     }
+    if (margin_out)  // a window whose best is another (template, angle) than the pixel's winner
+      for (int b = 0; b < ws.W; ++b) {
+        int i = b % ws.bx, j = b / ws.bx;
+        for (size_t k = 0; k < L2; ++k) {
+          if (carg[(size_t)b * L2 + k] < 0) continue;
+          double s = sd[(size_t)b * L2 + k];
+          int cx = ws.offx[i] + (int)(k % l), cy = ws.offy[j] + (int)(k / l);
+          if (cx >= nx || cy >= ny || s <= 0) continue;
+          size_t q = (size_t)cy * nx + cx;
+          if (carg[(size_t)b * L2 + k] != Zarg[q])
+            Zalt[q] = std::max(Zalt[q], (cmax[(size_t)b * L2 + k] - mu[(size_t)b * L2 + k]) / s);
+        }
+      }
     std::vector<size_t> cand;
     for (int y = 0; y < ny; ++y)
       for (int x = 0; x < nx; ++x) {
@@ -795,15 +865,20 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
     std::stable_sort(cand.begin(), cand.end(), [&](size_t u, size_t v) { return Z[u] > Z[v]; });
     const double r2 = (double)c.exclusion_radius * c.exclusion_radius;
     std::vector<size_t> acc;
-    for (size_t q : cand) {
-      if ((int)acc.size() >= c.topk) break;
+    auto excluded = [&](size_t q, size_t upto) {
       int x = q % nx, y = q / nx;
-      bool ok = true;
-      for (size_t a2 : acc) {
-        double dx = x - (int)(a2 % nx), dy = y - (int)(a2 / nx);
-        if (dx * dx + dy * dy <= r2) { ok = false; break; }
+      for (size_t u = 0; u < upto; ++u) {
+        double dx = x - (int)(acc[u] % nx), dy = y - (int)(acc[u] / nx);
+        if (dx * dx + dy * dy <= r2) return true;
       }
-      if (!ok) continue;
+      return false;
+    };
+    size_t next_rank = cand.size();  // rank of the first candidate a (K+1)-th pick would take
+    for (size_t rk = 0; rk < cand.size(); ++rk) {
+      size_t q = cand[rk];
+      if (excluded(q, acc.size())) continue;
+      if ((int)acc.size() >= c.topk) { next_rank = rk; break; }
+      int x = q % nx, y = q / nx;
       acc.push_back(q);
       gisspa_pick pk{};
       pk.score = Z[q];
@@ -814,6 +889,37 @@ int orc_search_norm(const gisspa_config* cin, const gisspa_ctf* ctf, const float
       pk.angle = cur_e; pk.theta = angles[a];
       pk.template_id = n; pk.window = Zwin[q]; pk.angle_index = a; pk.chunk = (int)acc.size() - 1;
       out.push_back(pk);
+    }
+    if (margin_out) {
+      // position competitors: candidates within the radius of a pick that no earlier pick excluded
+      std::vector<double> pos_m(acc.size(), INFINITY);
+      const int rr = (int)std::ceil(c.exclusion_radius);
+      for (size_t u = 0; u < acc.size(); ++u) {
+        const int x = acc[u] % nx, y = acc[u] / nx;
+        for (int yy = std::max(0, y - rr); yy <= std::min(ny - 1, y + rr); ++yy)
+          for (int xx = std::max(0, x - rr); xx <= std::min(nx - 1, x + rr); ++xx) {
+            const size_t q = (size_t)yy * nx + xx;
+            double dx = xx - x, dy = yy - y;
+            if (q == acc[u] || dx * dx + dy * dy > r2) continue;
+            if (Zarg[q] < 0 || Z[q] < p.thresh || xx < p.d_m || xx >= nx - p.d_m || yy < p.d_m || yy >= ny - p.d_m)
+              continue;
+            if (excluded(q, u)) continue;
+            pos_m[u] = std::min(pos_m[u], (double)Z[acc[u]] - (double)Z[q]);
+          }
+      }
+      for (size_t u = 0; u < acc.size(); ++u) {
+        double m = std::min(pos_m[u], (double)Z[acc[u]] - Zalt[acc[u]]);
+        if (u + 1 == acc.size() && next_rank < cand.size()) m = std::min(m, (double)Z[acc[u]] - Z[cand[next_rank]]);
+        margins.push_back(m);
+      }
+    }
+  }
+  if (margin_out && !margins.empty()) std::memcpy(margin_out, margins.data(), sizeof(double) * std::min(cap, margins.size()));
+  if (n_near) {
+    *n_near = near.size();
+    if (near_out && near.size() <= near_cap && !near.empty()) {
+      std::memcpy(near_out, near.data(), sizeof(gisspa_pick) * near.size());
+      std::memcpy(near_margin, near_m.data(), sizeof(double) * near.size());
     }
   }
   *n_out = out.size();
@@ -839,9 +945,13 @@ int orc_tiles(int width, int height, int tile, int* ulx, int* uly, int cap) {
 
 // Full norm_type=0 search (SearchNoNorm::work, nonorm.cu:559-589) over the tiles of one
 // micrograph.  max_angles > 0 restricts the angle loop (timing samples only).
+//  margin_out (optional, cap doubles): per pick, the smaller of (its score minus the best score
+//  of another window with a valid centre) and (its score minus the score its window's next best
+//  pixel would give, (peak - second peak) / sd); below twice a comparison tolerance the pick may
+//  legitimately land on the other window or pixel in FP32.
 int orc_search_nonorm(const gisspa_config* cin, const gisspa_ctf* ctf, const float* image, int nx, int ny,
                       const float* stack, int nt, int tw, int th, gisspa_pick* picks, size_t cap,
-                      size_t* n_out, int max_angles) {
+                      size_t* n_out, int max_angles, double* margin_out) {
   int st = validate(cin, nx, ny, nt, tw, th);
   if (st) return st;
   gisspa_config c = *cin;
@@ -857,6 +967,12 @@ int orc_search_nonorm(const gisspa_config* cin, const gisspa_ctf* ctf, const flo
   std::vector<float> angles = angle_list(c.phistep);
   int n_ang = max_angles > 0 ? std::min<int>(max_angles, angles.size()) : (int)angles.size();
   std::vector<gisspa_pick> out;
+  std::vector<double> margins;
+  // top-K per template (no counterpart in the reference): every (tile, angle, window) peak with a
+  // valid centre and score >= threshold, centre in micrograph coordinates, then greedy selection
+  struct Cand { double score; float x, y; int tile, angle, window; double pos_margin; };
+  const bool topk = c.pick_mode == GISSPA_PICK_TOPK;
+  std::vector<std::vector<Cand>> cands(topk ? nt : 0);
   for (int tI = 0; tI < ntiles && tI < 4096; ++tI) {
     std::vector<double> tile((size_t)ts * ts);
     for (int r = 0; r < ts; ++r)
@@ -898,9 +1014,10 @@ int orc_search_nonorm(const gisspa_config* cin, const gisspa_ctf* ctf, const flo
         }
       }
       std::vector<float> best_s(nt, 0.f), best_x(nt, 0.f), best_y(nt, 0.f);
+      std::vector<double> second_s(nt, 0.0), best_pm(nt, INFINITY);  // margins only
       for (int b = 0; b < W; ++b) {
         int i = b % bx, j = b / bx;
-        std::vector<double> peaks(nt), pos(nt), sums(nt), sum2s(nt);
+        std::vector<double> peaks(nt), pos(nt), sums(nt), sum2s(nt), peak2(nt);
 #pragma omp parallel
         {
           std::vector<cd> buf;
@@ -909,7 +1026,7 @@ int orc_search_nonorm(const gisspa_config* cin, const gisspa_ctf* ctf, const flo
           for (int n = 0; n < nt; ++n) {
             correlate(I.data() + (size_t)b * L2, Tsp.data() + (size_t)n * L2, l, cc.data(), buf);
             // get_peak_and_SUM (kernels.cu:725-763) + host merge (nonorm.cu:498-506)
-            double pk = 0, ps = 0, s = 0, s2 = 0;
+            double pk = 0, ps = 0, s = 0, s2 = 0, v1 = -INFINITY, v2 = -INFINITY;
             for (size_t ch = 0; ch < L2 / 256; ++ch) {
               double cb = 0;
               unsigned cl = 0;
@@ -920,10 +1037,11 @@ int orc_search_nonorm(const gisspa_config* cin, const gisspa_ctf* ctf, const flo
                 s += v; s2 += v * v;
                 if (x < p.d_m / 4 || x > l - p.d_m / 4 || y < p.d_m / 4 || y > l - p.d_m / 4) v = 0;
                 if (t == 0 || chunk_better(v, t, cb, cl)) { cb = v; cl = t; }
+                if (v > v1) { v2 = v1; v1 = v; } else if (v > v2) { v2 = v; }
               }
               if (pk < cb) { pk = cb; ps = (double)(ch * 256 + cl); }
             }
-            peaks[n] = pk; pos[n] = ps; sums[n] = s; sum2s[n] = s2;
+            peaks[n] = pk; pos[n] = ps; sums[n] = s; sum2s[n] = s2; peak2[n] = v2;
           }
         }
         // score = peak / sd of the map without the peak (nonorm.cu:509-533)
@@ -937,11 +1055,23 @@ int orc_search_nonorm(const gisspa_config* cin, const gisspa_ctf* ctf, const flo
                            (cy - l / 2) * std::sin(e * REF_PI / 180) + l / 2;
           double centery = j * (l - c.overlap) + (cy - l / 2) * std::cos(e * REF_PI / 180) -
                            (cx - l / 2) * std::sin(e * REF_PI / 180) + l / 2;
-          if (best_s[n] < (float)score && centerx >= 0 && centerx < ts && centery >= 0 && centery < ts) {
+          const bool valid = centerx >= 0 && centerx < ts && centery >= 0 && centery < ts;
+          if (topk) {
+            if (valid && (float)score >= p.thresh)
+              cands[n].push_back(Cand{score, (float)(ulx[tI] + centerx), (float)(uly[tI] + centery), tI, a, b,
+                                      sdv == 0 ? 0.0 : (peaks[n] - peak2[n]) / sdv});
+            continue;
+          }
+          if (best_s[n] < (float)score && valid) {
+            second_s[n] = best_s[n];
             best_s[n] = (float)score; best_x[n] = (float)centerx; best_y[n] = (float)centery;
+            best_pm[n] = sdv == 0 ? 0.0 : (peaks[n] - peak2[n]) / sdv;
+          } else if (valid) {
+            second_s[n] = std::max(second_s[n], score);
           }
         }
       }
+      if (topk) continue;
       // OutputScore (nonorm.cu:539-557): one line per template with score >= threshold
       for (int n = 0; n < nt; ++n)
         if (best_s[n] >= p.thresh) {
@@ -950,9 +1080,50 @@ int orc_search_nonorm(const gisspa_config* cin, const gisspa_ctf* ctf, const flo
           pk.angle = e; pk.theta = e; pk.template_id = n; pk.window = -1; pk.tile = tI;
           pk.angle_index = a; pk.chunk = -1;
           out.push_back(pk);
+          margins.push_back(std::min((double)best_s[n] - second_s[n], best_pm[n]));
         }
     }
   }
+  for (int n = 0; topk && n < nt; ++n) {
+    std::vector<Cand>& cd_ = cands[n];
+    std::stable_sort(cd_.begin(), cd_.end(), [](const Cand& u, const Cand& v) { return u.score > v.score; });
+    const double r2 = (double)c.exclusion_radius * c.exclusion_radius;
+    std::vector<size_t> taken;
+    auto near_taken = [&](const Cand& q, size_t upto) {
+      for (size_t u = 0; u < upto; ++u) {
+        const double dx = (double)q.x - cd_[taken[u]].x, dy = (double)q.y - cd_[taken[u]].y;
+        if (dx * dx + dy * dy <= r2) return true;
+      }
+      return false;
+    };
+    size_t next = cd_.size();
+    for (size_t k = 0; k < cd_.size(); ++k) {
+      if (near_taken(cd_[k], taken.size())) continue;
+      if ((int)taken.size() >= c.topk) { next = k; break; }
+      taken.push_back(k);
+    }
+    for (size_t u = 0; u < taken.size(); ++u) {
+      const Cand& q = cd_[taken[u]];
+      gisspa_pick pk{};
+      pk.score = (float)q.score; pk.x = q.x; pk.y = q.y;
+      pk.angle = angles[q.angle]; pk.theta = angles[q.angle]; pk.template_id = n; pk.window = q.window;
+      pk.tile = q.tile; pk.angle_index = q.angle; pk.chunk = (int)u;
+      out.push_back(pk);
+      // margin: the peak's own pixel competitor, the other not-yet-excluded peaks within the
+      // radius, and for the last pick the peak a larger K would take next
+      double m = q.pos_margin;
+      for (size_t k = 0; k < cd_.size(); ++k) {
+        if (k == taken[u]) continue;
+        const double dx = (double)cd_[k].x - q.x, dy = (double)cd_[k].y - q.y;
+        if (dx * dx + dy * dy > r2 || near_taken(cd_[k], u)) continue;
+        m = std::min(m, std::fabs(q.score - cd_[k].score));
+      }
+      if (u + 1 == taken.size() && next < cd_.size()) m = std::min(m, q.score - cd_[next].score);
+      margins.push_back(m);
+    }
+  }
+  if (margin_out && !margins.empty())
+    std::memcpy(margin_out, margins.data(), sizeof(double) * std::min(cap, margins.size()));
   *n_out = out.size();
   if (out.size() > cap) return GISSPA_ERR_CAPACITY;
   if (!out.empty()) std::memcpy(picks, out.data(), sizeof(gisspa_pick) * out.size());

@@ -36,10 +36,10 @@ def load():
         lib.orc_rotated_spectrum.argtypes = [C.POINTER(gisspa.Config), C.POINTER(gisspa.Ctf), _P, C.c_float, _P]
         lib.orc_search_norm.argtypes = [C.POINTER(gisspa.Config), C.POINTER(gisspa.Ctf), _P, C.c_int, C.c_int, _P,
                                         C.c_int, C.c_int, C.c_int, _P, C.c_size_t, C.POINTER(C.c_size_t), _P,
-                                        C.c_int, C.c_int]
+                                        C.c_int, C.c_int, _P, _P, _P, C.c_size_t, C.POINTER(C.c_size_t)]
         lib.orc_search_nonorm.argtypes = [C.POINTER(gisspa.Config), C.POINTER(gisspa.Ctf), _P, C.c_int, C.c_int,
                                           _P, C.c_int, C.c_int, C.c_int, _P, C.c_size_t, C.POINTER(C.c_size_t),
-                                          C.c_int]
+                                          C.c_int, _P]
         lib.orc_tiles.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, C.c_int]
         lib.orc_num_threads.restype = C.c_int
         lib.orc_project3d.argtypes = [_P, C.c_int, C.c_int, C.c_int, _P, C.c_int, C.c_int, _P]
@@ -95,32 +95,45 @@ def rotated_spectrum(cfg, ctf, prep: np.ndarray, theta: float) -> np.ndarray:
 
 
 def search(cfg, ctf, image: np.ndarray, stack: np.ndarray, cap: int = 1 << 20, want_stats: bool = False,
-           max_templates: int = 0, max_angles: int = 0):
-    """Full search; returns picks (PICK_DTYPE) and, for norm_type=1 with want_stats, (mu, sigma) maps."""
+           max_templates: int = 0, max_angles: int = 0, want_margins: bool = False):
+    """Full search; returns picks (PICK_DTYPE) and, for norm_type=1 with want_stats, (mu, sigma) maps.
+    want_margins: also returns each pick's decision margin in z (see orc_search_norm /
+    orc_search_nonorm) and, for chunk picks, the near misses (picks, margins) that FP32 rounding
+    could turn into picks: the result is then (picks, margins, near, near_margins[, stats])."""
     image = np.ascontiguousarray(image, dtype=np.float32)
     stack = np.ascontiguousarray(stack, dtype=np.float32)
     ny, nx = image.shape
     n, th, tw = stack.shape
     out = np.zeros(cap, dtype=gisspa.PICK_DTYPE)
     nout = C.c_size_t(0)
+    margins = np.zeros(cap, dtype=np.float64) if want_margins else None
+    near_cap = 1 << 16
+    near = np.zeros(near_cap, dtype=gisspa.PICK_DTYPE) if want_margins else None
+    near_m = np.zeros(near_cap, dtype=np.float64) if want_margins else None
+    n_near = C.c_size_t(0)
     lib = load()
+    ptr = lambda a: a.ctypes.data if a is not None else None
     if cfg.norm_type:
         l = cfg.window_size
         W = len(window_offsets(nx, l, cfg.overlap)) * len(window_offsets(ny, l, cfg.overlap))
         stats = np.zeros((W, l, l, 2), dtype=np.float64) if want_stats else None
         st = lib.orc_search_norm(C.byref(cfg), C.byref(ctf), image.ctypes.data, nx, ny, stack.ctypes.data, n, tw, th,
-                                 out.ctypes.data, cap, C.byref(nout),
-                                 stats.ctypes.data if stats is not None else None, max_templates, max_angles)
+                                 out.ctypes.data, cap, C.byref(nout), ptr(stats), max_templates, max_angles,
+                                 ptr(margins), ptr(near), ptr(near_m), near_cap, C.byref(n_near))
     else:
         stats = None
         st = lib.orc_search_nonorm(C.byref(cfg), C.byref(ctf), image.ctypes.data, nx, ny, stack.ctypes.data, n, tw,
-                                   th, out.ctypes.data, cap, C.byref(nout), max_angles)
+                                   th, out.ctypes.data, cap, C.byref(nout), max_angles, ptr(margins))
     if st == gisspa.ERR_CAPACITY:
         return search(cfg, ctf, image, stack, cap=int(nout.value), want_stats=want_stats,
-                      max_templates=max_templates, max_angles=max_angles)
+                      max_templates=max_templates, max_angles=max_angles, want_margins=want_margins)
     if st != 0:
         raise RuntimeError(f"oracle status {st}")
+    assert n_near.value <= near_cap, "more near misses than the buffer holds"
     picks = out[: nout.value].copy()
+    if want_margins:
+        res = (picks, margins[: nout.value].copy(), near[: n_near.value].copy(), near_m[: n_near.value].copy())
+        return res + (stats,) if want_stats else res
     return (picks, stats) if want_stats else picks
 
 

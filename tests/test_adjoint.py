@@ -139,3 +139,34 @@ def test_gradients_match_fp64_oracle(searched):
         e1 = np.linalg.norm(ours[:3] - g_or[:3]) / max(np.linalg.norm(g_or[:3]), 1e-6)
         e2 = np.linalg.norm(ours[3:] - g_or[3:]) / max(np.linalg.norm(g_or[3:]), 1e-6)
         assert e1 < GRAD_RTOL and e2 < GRAD_RTOL, (ours, g_or, e1, e2)
+
+
+@pytest.mark.parametrize("spec,tol", [(gisspa.SPEC_FP16, 2e-3), (gisspa.SPEC_BF16, 2e-2)])
+def test_half_precision_template_adjoint(spec, tol):
+    """The FP16 / BF16 template forms: the adjoint reads the prepared templates and their CTF
+    derivatives rounded to that precision.  Its scores stay within the precision's tolerance of
+    the FP32 form's, and its gradient is the derivative of its own scores (central differences,
+    as the FP32 harness above)."""
+    img, tmpl, ctf, cfg = small_case("norm_l256_w9")
+    cfg = cfg.copy(pick_mode=gisspa.PICK_TOPK, topk=12, exclusion_radius=30.0, threshold=2.0)
+    s32 = gisspa.Searcher(cfg)
+    s32.set_templates(tmpl)
+    picks = s32.search(img, ctf)[:6]
+    s16 = gisspa.Searcher(cfg.copy(spectrum_precision=spec))
+    s16.set_templates(tmpl)
+    s16.search(img, ctf)
+    base = np.stack([np.full(len(picks), 0.31), np.full(len(picks), -0.23), picks["theta"] + 1.7], 1).astype(np.float32)
+    g32 = s32.score_grad(picks, base, ctf)
+    g16 = s16.score_grad(picks, base, ctf)
+    assert np.allclose(g16["score"], g32["score"], rtol=tol), (g16["score"], g32["score"])
+    adj = np.stack([g16["d_dx"], g16["d_dy"], g16["d_theta"]], 1).astype(np.float64)
+    fd = np.zeros_like(adj)
+    for k in range(3):
+        d = np.zeros_like(base)
+        d[:, k] = FD_H
+        hi, lo = base + d, base - d
+        step = hi[:, k].astype(np.float64) - lo[:, k].astype(np.float64)
+        fd[:, k] = (_score(s16, picks, hi, ctf) - _score(s16, picks, lo, ctf)) / step
+    for i in range(len(picks)):
+        err = np.linalg.norm(adj[i] - fd[i]) / max(np.linalg.norm(fd[i]), 1e-6)
+        assert err < FD32_RTOL, (i, adj[i], fd[i], err)

@@ -13,7 +13,7 @@ import pytest
 
 import gisspa
 import oracle
-from parity import compare_chunk_picks, small_case
+from parity import check_chunk_picks, small_case
 
 pytestmark = pytest.mark.gpu
 
@@ -81,8 +81,7 @@ def test_small_and_ragged_micrographs_match_the_oracle(shape, threshold):
     s = gisspa.Searcher(cfg)
     s.set_templates(tmpl)
     g = s.search(canvas, ctf)
-    o = oracle.search(cfg, ctf, canvas, tmpl)
-    rep = compare_chunk_picks(g, o, cfg.threshold)
+    o, m, near, nm = oracle.search(cfg, ctf, canvas, tmpl, want_margins=True)
+    rep = check_chunk_picks(g, o, m, near, nm, cfg.threshold)
     assert len(o) > 0
-    assert rep["missing"] == 0 and rep["extra"] == 0 and rep["score_bad"] == 0, rep
-    assert rep["pos_bad"] <= max(1, len(o) // 200), rep
+    assert not rep["failures"], rep
