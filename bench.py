@@ -55,6 +55,8 @@ def args_parse():
     ap.add_argument("--form", default="plain", choices=list(FORMS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-precision-check", action="store_true",
+                    help="skip the untimed FP32 / BF16 top-K searches that measure the chosen form's score error")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="--impl reference: skip timing the reference's own CUDA build beside the oracle")
     ap.add_argument("--eager", action="store_true",
@@ -181,6 +183,32 @@ def oracle_rate(case, cfg, n_angles: int):
     nt = case.templates.shape[0]
     mic_s = prep + per_rot * nt * n_angles
     return 1.0 / mic_s, oracle.num_threads(), sum(t), per_rot, prep
+
+
+def precision_check(case, ctf, d_img, nx, ny, wl, chosen_name, chosen_picks, local, out) -> dict:
+    """Peak-score error of the reduced-precision template forms against the FP32 form of the
+    same one-sweep top-K search on the same micrograph (untimed): the picks of the timed chosen
+    form and of one BF16 search, each matched to the FP32 picks by (x, y, template, angle)."""
+    def run(spec):
+        p = dict(synth.SEARCH_PARAMS[wl])
+        p.update(spectrum_precision=spec, pick_mode=gisspa.PICK_TOPK)
+        s = gisspa.Searcher(gisspa.Config.default(**p), local)
+        s.set_templates(case.templates)
+        n = s.search_device(d_img.data_ptr(), nx, ny, ctf, out)
+        s.close()
+        return out[:n].copy()
+
+    ref = run(gisspa.SPEC_FP32)
+    key = lambda q: (float(q["x"]), float(q["y"]), int(q["template_id"]), int(q["angle_index"]))
+    R = {key(q): float(q["score"]) for q in ref}
+    res = {"picks_fp32": len(ref)}
+    for name, picks in ((chosen_name, chosen_picks), ("bf16_topk", run(gisspa.SPEC_BF16))):
+        rel = [abs(float(q["score"]) - R[key(q)]) / abs(R[key(q)]) for q in picks if key(q) in R]
+        res[name] = {"picks": len(picks), "same_picks": len(rel),
+                     "max_rel": float(max(rel)) if rel else None,
+                     "p99_rel": float(np.quantile(rel, 0.99)) if rel else None,
+                     "median_rel": float(np.median(rel)) if rel else None}
+    return res
 
 
 def reference_cuda_timing(wl: str) -> dict:
@@ -431,13 +459,17 @@ def main():
         if rank != 0:
             return
         case = synth.make_case(**data)
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle
+
+        ctf0 = gisspa.Ctf(case.defocus, case.dfdiff, case.dfang)
+        for _ in range(a.warmup):  # warm-up: threads and caches (one template at one angle)
+            oracle.search(cfg, ctf0, case.image, case.templates, max_templates=1, max_angles=1)
         steps, step_s = [], []
-        for i in range(a.warmup + a.steps):
+        for i in range(a.steps):
             t0 = time.perf_counter()
-            r = oracle_rate(case, cfg, angles)
-            if i >= a.warmup:
-                steps.append(r)
-                step_s.append(time.perf_counter() - t0)
+            steps.append(oracle_rate(case, cfg, angles))
+            step_s.append(time.perf_counter() - t0)
         rate = float(np.mean([s[0] for s in steps]))
         cores = steps[0][1]
         sample = (f"FP64 oracle, {wl}: 4 and 10 templates x 1 angle over all windows (both sweeps), "
@@ -578,10 +610,14 @@ def main():
             torch.distributed.all_reduce(t2, op=torch.distributed.ReduceOp.MAX)
         v2 = world * a.steps / (float(t2.item()) / 1000.0)
         st2 = s2.stats()
+        chosen_picks = out[:n2].copy()
         chosen = {"form": a.chosen, "value": v2, "unit": "micrographs/s", "ms_per_step": float(t2.item()) / a.steps,
                   "vs_plain": v2 / value, "picks_per_step": int(n2), "launch_pair_us": st2.corr_pair_us,
                   "pairs_per_launch": st2.pairs_per_launch}
         s2.close()
+        if not a.no_precision_check:
+            chosen["score_err_vs_fp32"] = precision_check(case, ctf, d_img, nx, ny, wl, a.chosen, chosen_picks, local,
+                                                          out)
 
     res = None
     if rank == 0:

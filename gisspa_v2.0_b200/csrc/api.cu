@@ -86,6 +86,7 @@ int gisspa_create(const gisspa_config* cfg, int device, gisspa_handle** out) {
     GISSPA_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
     GISSPA_CUDA(cudaEventCreateWithFlags(&h->ev_in, cudaEventDisableTiming));
     GISSPA_CUDA(cudaEventCreateWithFlags(&h->ev_stats, cudaEventDisableTiming));
+    GISSPA_CUDA(cudaEventCreateWithFlags(&h->ev_next, cudaEventDisableTiming));
     for (auto& e : h->ev) GISSPA_CUDA(cudaEventCreate(&e));
     for (auto& r : h->sev)
       for (auto& e : r) GISSPA_CUDA(cudaEventCreate(&e));

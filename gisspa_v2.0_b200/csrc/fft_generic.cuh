@@ -8,6 +8,8 @@
 // rows -> transpose -> rows (-> transpose).  All transforms are unnormalised.
 #pragma once
 
+#include <utility>
+
 #include <atomic>
 #include <map>
 #include <memory>
@@ -52,6 +54,10 @@ class DevBuf {
   template <typename T>
   T* as() const { return static_cast<T*>(p_); }
   size_t size() const { return n_; }
+  void swap(DevBuf& o) noexcept {
+    std::swap(p_, o.p_);
+    std::swap(n_, o.n_);
+  }
 
  private:
   void* p_ = nullptr;

@@ -331,8 +331,12 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   static const Cand c512[] = {{8, 8}, {12, 8}, {6, 12}, {8, 12}, {4, 16}, {6, 16}, {16, 6}, {24, 4}};
   static const Cand c1024[] = {{6, 4}, {4, 6}, {3, 8}, {2, 12}, {4, 8}, {8, 3}, {2, 16}};
   static const Cand c256[] = {{16, 8}, {32, 8}, {8, 16}, {16, 16}, {64, 4}};
-  const Cand* cb = l == 512 ? c512 : l == 1024 ? c1024 : c256;
-  const size_t nc = l == 512 ? std::size(c512) : l == 1024 ? std::size(c1024) : std::size(c256);
+  static const Cand c320[] = {{12, 8}, {16, 8}, {8, 16}, {24, 8}, {16, 16}, {32, 4}};
+  const Cand* cb = l == 512 ? c512 : l == 1024 ? c1024 : l == 320 ? c320 : c256;
+  const size_t nc = l == 512    ? std::size(c512)
+                    : l == 1024 ? std::size(c1024)
+                    : l == 320  ? std::size(c320)
+                                : std::size(c256);
   std::vector<Cand> cands(cb, cb + nc);
   int maxE = 1, maxDE = 1;
   for (auto& cd : cands) {
@@ -471,14 +475,23 @@ void norm_prepare(Ctx& c, const float* d_img, int nx, int ny, NormRun& r) {
   GISSPA_CUDA(cudaEventRecord(h->ev[0], c.s));
   // LoadImage statistics on the side stream (the serial FP32 form occupies one SM for
   // ~4 ns per pixel) while the templates are prepared on the main stream
-  float* stats = buf<float>(h->stats, 4);
-  double* scr = buf<double>(h->scratch, 16);
-  GISSPA_CUDA(cudaEventRecord(h->ev_in, c.s));
-  GISSPA_CUDA(cudaStreamWaitEvent(h->side, h->ev_in, 0));
-  image_stats(d_img, nx, ny, (cfg.quirks & GISSPA_QUIRK_OUTLIER_FP32_SERIAL) != 0, stats, scr, h->side);
-  GISSPA_CUDA(cudaEventRecord(h->ev_stats, h->side));
+  const bool prefetched = h->next_dev == d_img && h->next_nx == nx && h->next_ny == ny;
+  h->next_dev = nullptr;
+  if (prefetched) {
+    // a batch started this micrograph's statistics during the previous one's sweeps
+    h->stats.swap(h->stats_next);
+    h->scratch.swap(h->scratch_next);
+  } else {
+    float* st0 = buf<float>(h->stats, 4);
+    double* scr = buf<double>(h->scratch, 16);
+    GISSPA_CUDA(cudaEventRecord(h->ev_in, c.s));
+    GISSPA_CUDA(cudaStreamWaitEvent(h->side, h->ev_in, 0));
+    image_stats(d_img, nx, ny, (cfg.quirks & GISSPA_QUIRK_OUTLIER_FP32_SERIAL) != 0, st0, scr, h->side);
+    GISSPA_CUDA(cudaEventRecord(h->ev_stats, h->side));
+  }
+  float* stats = h->stats.as<float>();
   prepare_templates(c);
-  GISSPA_CUDA(cudaStreamWaitEvent(c.s, h->ev_stats, 0));
+  GISSPA_CUDA(cudaStreamWaitEvent(c.s, prefetched ? h->ev_next : h->ev_stats, 0));
   // micrograph
   float2* G = buf<float2>(h->img_c, r.N);
   image_load(d_img, r.N, stats, true, cfg.invert != 0, G, c.s);
@@ -800,6 +813,11 @@ void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_
   norm_prepare(c, d_img, nx, ny, r);
   const int A = (int)r.angles.size();
   norm_sweep1(c, r, 0, A);
+  if (h->after_sweep1) {  // the sweep is queued: the host is free until the picks are read
+    std::function<void()> f = std::move(h->after_sweep1);
+    h->after_sweep1 = nullptr;
+    f();
+  }
   norm_stats(c, r);
   GISSPA_CUDA(cudaEventRecord(h->ev[2], c.s));
   if (!r.topk) {
@@ -1486,16 +1504,47 @@ int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx
   std::vector<gisspa_pick> all, one;
   offsets[0] = 0;
   gisspa_stats total{};
+  h->next_dev = nullptr;
+  // Micrographs alternate between two device buffers.  While micrograph i's first sweep runs
+  // (norm_type=1), the host uploads micrograph i+1 into the other buffer on the side stream and
+  // queues its LoadImage statistics (one thread, ~65 ms at 4096^2) there; search i+1 then starts
+  // from them.  Buffer i+1 last held micrograph i-1, whose search has returned.
+  gisspa::DevBuf* bufs[2] = {&h->img_in, &h->img_next};
   for (int i = 0; i < n; ++i) {
     one.clear();
     int st = guarded(h, [&] {
       GISSPA_CUDA(cudaSetDevice(h->device));
+      gisspa::DevBuf& cur = *bufs[i & 1];
       const size_t bytes = sizeof(float) * (size_t)nx[i] * ny[i];
-      h->img_in.ensure(bytes);
-      GISSPA_CUDA(cudaMemcpyAsync(h->img_in.as<float>(), images[i], bytes, cudaMemcpyHostToDevice, h->stream));
-      run_search(h, h->img_in.as<float>(), nx[i], ny[i], ctfs[i], one);
+      if (h->next_dev == nullptr || h->next_dev != cur.as<float>()) {
+        h->next_dev = nullptr;
+        cur.ensure(bytes);
+        GISSPA_CUDA(cudaMemcpyAsync(cur.as<float>(), images[i], bytes, cudaMemcpyHostToDevice, h->stream));
+      }
+      if (i + 1 < n && h->cfg.norm_type != 0) {
+        h->after_sweep1 = [h, &bufs, i, images, nx, ny] {
+          gisspa::DevBuf& nb = *bufs[(i + 1) & 1];
+          const size_t b2 = sizeof(float) * (size_t)nx[i + 1] * ny[i + 1];
+          float* dst = static_cast<float*>(nb.ensure(b2));
+          float* st1 = buf<float>(h->stats_next, 4);
+          double* scr = buf<double>(h->scratch_next, 16);
+          GISSPA_CUDA(cudaMemcpyAsync(dst, images[i + 1], b2, cudaMemcpyHostToDevice, h->side));
+          image_stats(dst, nx[i + 1], ny[i + 1], (h->cfg.quirks & GISSPA_QUIRK_OUTLIER_FP32_SERIAL) != 0, st1, scr,
+                      h->side);
+          GISSPA_CUDA(cudaEventRecord(h->ev_next, h->side));  // the next search waits on it
+          h->next_dev = dst;
+          h->next_nx = nx[i + 1];
+          h->next_ny = ny[i + 1];
+        };
+      }
+      run_search(h, cur.as<float>(), nx[i], ny[i], ctfs[i], one);
+      h->after_sweep1 = nullptr;
     });
-    if (st) return st;
+    if (st) {
+      h->after_sweep1 = nullptr;
+      h->next_dev = nullptr;
+      return st;
+    }
     total.ms_total += h->st.ms_total;
     total.ms_prep += h->st.ms_prep;
     total.ms_sweep1 += h->st.ms_sweep1;

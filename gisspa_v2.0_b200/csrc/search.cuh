@@ -1,6 +1,7 @@
 // search.cuh — the search handle and the per-micrograph orchestration.
 #pragma once
 
+#include <functional>
 #include <map>
 #include <new>
 #include <string>
@@ -84,6 +85,13 @@ struct gisspa_handle {
   // d(prepared template)/dpsi, window RMS factors and sums
   gisspa::DevBuf tw_spec, tmpl_m, dtab, dprep, win_m, win_sum, grad_in, grad_out;
   gisspa::DevBuf prep_lp, dprep_lp;  // adjoint templates at the FP16 / BF16 template precision
+  // batches: the next micrograph's upload and LoadImage statistics run while the current one's
+  // first sweep is on the GPU (gisspa_search_batch)
+  gisspa::DevBuf img_next, stats_next, scratch_next;
+  cudaEvent_t ev_next = nullptr;
+  const float* next_dev = nullptr;  // device image whose statistics wait in stats_next
+  int next_nx = 0, next_ny = 0;
+  std::function<void()> after_sweep1;
   bool keep_whitened = false;
   int last_nx = 0, last_ny = 0, last_W = 0, last_bx = 0;
   gisspa_ctf last_ctf{};
@@ -122,6 +130,7 @@ struct gisspa_handle {
     for (auto& r : qev)
       for (auto& e : r)
         if (e) cudaEventDestroy(e);
+    if (ev_next) cudaEventDestroy(ev_next);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_stats) cudaEventDestroy(ev_stats);
     if (side) cudaStreamDestroy(side);

@@ -156,6 +156,9 @@ WORKLOADS = {
     # 24 templates, 4 angles
     "whole_2048_t24": dict(shape=(2048, 2048), n_particles=40, snr=0.05, n_templates=24, tsize=180, seed=3,
                            defocus=1.7, dfdiff=0.1, dfang=30.0),
+    # profiling case at the reference's default window size 320 (overlap 120)
+    "whole_2048_t24_w320": dict(shape=(2048, 2048), n_particles=40, snr=0.05, n_templates=24, tsize=180, seed=3,
+                                defocus=1.7, dfdiff=0.1, dfang=30.0),
 }
 
 SEARCH_PARAMS = {
@@ -172,6 +175,8 @@ SEARCH_PARAMS = {
                      diameter=150.0, threshold=7.0, window_size=512, overlap=200, norm_type=1),
     "whole_2048_t24": dict(angpix=1.0, phistep=90.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                            diameter=140.0, threshold=7.0, window_size=512, overlap=192, norm_type=1),
+    "whole_2048_t24_w320": dict(angpix=1.0, phistep=90.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                                diameter=140.0, threshold=7.0, window_size=320, overlap=120, norm_type=1),
 }
 
 

@@ -33,6 +33,11 @@ def test_reference_arm_line():
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    # the value is extrapolated from a bounded sample whose own time is ms_per_step
+    assert d["extrapolated"] is True and cb["extrapolated"] is True and cb["sample_s"] > 0
+    assert abs(d["ms_per_step"] - 1000.0 * cb["sample_s"]) < 1e-6 * d["ms_per_step"]
+    # no GPU here: the reference CUDA build's timing says why it is absent
+    assert "unavailable" in d["reference_cuda"]
 
 
 def test_reference_arm_other_ranks_print_nothing():
@@ -41,6 +46,6 @@ def test_reference_arm_other_ranks_print_nothing():
 
 
 def test_reference_arm_unavailable_workloads():
-    for wl in ("batch_c3", "project_c5"):
+    for wl in ("batch_c3", "project_c5", "adjoint_c4"):
         d = last_json(run(["--impl", "reference", "--workload", wl, "--steps", "1", "--warmup", "0"]))
         assert d["impl"] == "reference" and d["unavailable"]

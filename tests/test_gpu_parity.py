@@ -191,14 +191,21 @@ def test_search_host_and_device_paths_agree():
 
 
 def test_batch_matches_single_searches():
+    """A batch (each micrograph's upload and statistics overlapped with the previous one's
+    sweep, in two alternating buffers) gives the single searches' picks bit for bit, across
+    uneven sizes and CTFs."""
     img, tmpl, ctf, cfg = small_case("norm_l256_w9")
     img2 = np.ascontiguousarray(img[:, ::-1])
+    img3 = np.ascontiguousarray(np.concatenate([img, img[:200]], axis=0)[:, :448])
+    ctf3 = gisspa.Ctf(ctf.defocus + 0.3, ctf.dfdiff, ctf.dfang + 10.0)
     s = gisspa.Searcher(cfg)
     s.set_templates(tmpl)
-    one = [s.search(img, ctf), s.search(img2, ctf)]
-    both = s.search_batch([img, img2], [ctf, ctf])
-    for x, y in zip(one, both):
-        assert np.array_equal(x, y)
+    imgs, ctfs = [img, img2, img3, img], [ctf, ctf, ctf3, ctf]
+    one = [s.search(i, c) for i, c in zip(imgs, ctfs)]
+    batch = s.search_batch(imgs, ctfs)
+    assert len(batch) == len(one)
+    for x, y in zip(one, batch):
+        assert len(x) > 0 and np.array_equal(x, y)
 
 
 @pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4"])
