@@ -146,14 +146,35 @@ __device__ __forceinline__ double to_d(float v) { return (double)v; }
 __device__ __forceinline__ double to_d(__half v) { return (double)__half2float(v); }
 __device__ __forceinline__ double to_d(__nv_bfloat16 v) { return (double)__bfloat162float(v); }
 
+// Largest |value| of in[0, n), as the bits of a non-negative float (ordered like the value),
+// folded into *out.
+__global__ void abs_max_kernel(const float* __restrict__ in, long long n, unsigned* __restrict__ out) {
+  unsigned m = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = max(m, __float_as_uint(fabsf(in[i])));
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// Rounds to V.  FP16 has five exponent bits: the unnormalised real-space templates and their CTF
+// derivatives exceed its range, so every value is first scaled by one power of two that brings
+// the largest (*absmax, over both arrays) to [2^13, 2^14).  A common factor leaves the
+// normalised score and all its derivatives unchanged (the score is invariant to the template's
+// scale), and a power of two adds no rounding.  BF16 keeps FP32's exponent range (absmax null).
 template <typename V>
-__global__ void round_kernel(const float* __restrict__ in, long long n, V* __restrict__ out) {
+__global__ void round_kernel(const float* __restrict__ in, long long n, const unsigned* __restrict__ absmax,
+                             V* __restrict__ out) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  if constexpr (sizeof(V) == 2 && std::is_same<V, __half>::value)
-    out[i] = __float2half_rn(in[i]);
+  float scale = 1.f;
+  if (absmax) {
+    const float m = __uint_as_float(*absmax);
+    if (m > 0.f && isfinite(m)) scale = ldexpf(1.f, max(-120, min(120, 13 - ilogbf(m))));
+  }
+  if constexpr (std::is_same<V, __half>::value)
+    out[i] = __float2half_rn(in[i] * scale);
   else
-    out[i] = __float2bfloat16_rn(in[i]);
+    out[i] = __float2bfloat16_rn(in[i] * scale);
 }
 
 // V: storage type of the prepared templates and their CTF derivatives (float, __half or
@@ -283,11 +304,24 @@ void window_sums(const float* img, int nx, int ny, const int* offx, const int* o
   GISSPA_LAUNCH_CHECK();
 }
 
-void round_templates(const float* prep, long long n, int precision, void* out, cudaStream_t s) {
-  if (precision == GISSPA_SPEC_FP16)
-    round_kernel<__half><<<ceil_div(n, 256), 256, 0, s>>>(prep, n, static_cast<__half*>(out));
-  else
-    round_kernel<__nv_bfloat16><<<ceil_div(n, 256), 256, 0, s>>>(prep, n, static_cast<__nv_bfloat16*>(out));
+void round_templates(const float* prep, long long n1, const float* dprep, long long n2, int precision,
+                     unsigned* absmax, void* out1, void* out2, cudaStream_t s) {
+  if (precision == GISSPA_SPEC_FP16) {
+    GISSPA_CUDA(cudaMemsetAsync(absmax, 0, sizeof(unsigned), s));
+    abs_max_kernel<<<4 * 148, 256, 0, s>>>(prep, n1, absmax);
+    GISSPA_LAUNCH_CHECK();
+    abs_max_kernel<<<4 * 148, 256, 0, s>>>(dprep, n2, absmax);
+    GISSPA_LAUNCH_CHECK();
+    round_kernel<__half><<<ceil_div(n1, 256), 256, 0, s>>>(prep, n1, absmax, static_cast<__half*>(out1));
+    GISSPA_LAUNCH_CHECK();
+    round_kernel<__half><<<ceil_div(n2, 256), 256, 0, s>>>(dprep, n2, absmax, static_cast<__half*>(out2));
+  } else {
+    round_kernel<__nv_bfloat16><<<ceil_div(n1, 256), 256, 0, s>>>(prep, n1, nullptr,
+                                                                  static_cast<__nv_bfloat16*>(out1));
+    GISSPA_LAUNCH_CHECK();
+    round_kernel<__nv_bfloat16><<<ceil_div(n2, 256), 256, 0, s>>>(dprep, n2, nullptr,
+                                                                  static_cast<__nv_bfloat16*>(out2));
+  }
   GISSPA_LAUNCH_CHECK();
 }
 

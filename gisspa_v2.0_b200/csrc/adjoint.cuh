@@ -38,8 +38,11 @@ void ctf_dweight(float* dtab, int l, const DevParams& p, cudaStream_t s);
 void scale_by_table(const float2* F, const float* tab, const double* m, int nt, int l, float2* out, cudaStream_t s);
 void window_sums(const float* img, int nx, int ny, const int* offx, const int* offy, int bx, int nwin, int l,
                  const double* win_m, double* out, cudaStream_t s);
-// prep (n values) rounded to the template precision (1: FP16, 2: BF16) into out
-void round_templates(const float* prep, long long n, int precision, void* out, cudaStream_t s);
+// prep (n1 values) and dprep (n2) rounded to the template precision (1: FP16, 2: BF16) into out1,
+// out2; FP16 first scales both by one power of two that fits their largest value (absmax: one
+// unsigned of device scratch)
+void round_templates(const float* prep, long long n1, const float* dprep, long long n2, int precision,
+                     unsigned* absmax, void* out1, void* out2, cudaStream_t s);
 // out: n x 7 floats (z, dz/d(dx, dy, theta, dfu, dfv, dfang))
 void score_grads(const GradArgs& g, const GradPick* picks, int n, float* out, cudaStream_t s);
 

@@ -1129,11 +1129,10 @@ void adjoint_prepare(gisspa_handle* h, const gisspa_ctf& ctf) {
               h->last_W, l, h->win_m.as<double>(), buf<double>(h->win_sum, h->last_W), c.s);
   // the FP16 / BF16 template forms evaluate from templates stored at that precision
   const int prec = h->cfg.spectrum_precision;
-  if (prec != GISSPA_SPEC_FP32) {
-    round_templates(h->prep_real.as<float>(), (long long)nt * c.L2, prec, buf<__half>(h->prep_lp, (size_t)nt * c.L2),
-                    c.s);
-    round_templates(dprep, 3LL * nt * c.L2, prec, buf<__half>(h->dprep_lp, 3 * (size_t)nt * c.L2), c.s);
-  }
+  if (prec != GISSPA_SPEC_FP32)
+    round_templates(h->prep_real.as<float>(), (long long)nt * c.L2, dprep, 3LL * nt * c.L2, prec,
+                    buf<unsigned>(h->lp_scale, 1), buf<__half>(h->prep_lp, (size_t)nt * c.L2),
+                    buf<__half>(h->dprep_lp, 3 * (size_t)nt * c.L2), c.s);
 }
 
 void eval_grads(gisspa_handle* h, const std::vector<GradPick>& gp, std::vector<float>& out) {

@@ -84,7 +84,7 @@ struct gisspa_handle {
   // adjoint: whitened template spectra before weighting, RMS factors, dW/dpsi tables,
   // d(prepared template)/dpsi, window RMS factors and sums
   gisspa::DevBuf tw_spec, tmpl_m, dtab, dprep, win_m, win_sum, grad_in, grad_out;
-  gisspa::DevBuf prep_lp, dprep_lp;  // adjoint templates at the FP16 / BF16 template precision
+  gisspa::DevBuf prep_lp, dprep_lp, lp_scale;  // adjoint templates at the FP16 / BF16 precision
   // batches: the next micrograph's upload and LoadImage statistics run while the current one's
   // first sweep is on the GPU (gisspa_search_batch)
   gisspa::DevBuf img_next, stats_next, scratch_next;

@@ -168,6 +168,26 @@ Params make_params(const gisspa_config& c, const gisspa_ctf& ctf, int l) {
 
 // CTF_AST (kernels.cu:290-317): Hermitian fold, astigmatic defocus, amplitude contrast.
 double ctf_ast(int x1, int y1, int nx, int ny, const Params& p, int mode) {
+#ifdef ORC_CTF_REFERENCE_FP32
+  // The reference's own arithmetic (kernels.cu:290-317): float parameters and float sinf /
+  // cosf / atan2, with the double literals promoting the middle of the expressions.
+  {
+    const float apix = (float)p.apix, dfu = (float)p.dfu, dfv = (float)p.dfv, dfdiff = (float)p.dfdiff;
+    const float dfang = (float)p.dfang, lambda = (float)p.lambda, cs = (float)p.cs, ac = (float)p.ampconst;
+    y1 = x1 > nx / 2 ? ny - y1 : y1;
+    x1 = std::min(x1, nx - x1);
+    const float dx = (float)std::min(x1, nx - x1), dy = (float)(y1 - ny / 2);
+    const float ss = (dx * dx / (float)(nx * nx) + dy * dy / (float)(ny * ny)) / (apix * apix);
+    const float ag = std::atan2((float)(y1 - ny / 2), (float)x1);
+    const float df_ast = (float)(0.5 * (dfu + dfv + 2 * dfdiff * cosf((float)(2 * (dfang * REF_PI / 180 - ag)))));
+    const float gamma = (float)(-2 * REF_PI *
+                                (cs * 2.5e6 * lambda * lambda * lambda * ss * ss + df_ast * 5000.0 * lambda * ss));
+    const float v = sqrtf((float)(1.0 - ac * ac)) * sinf(gamma) + ac * cosf(gamma);
+    if (mode == 0) return v > 0 ? 1.0 : -1.0;
+    if (mode == 2) return std::fabs(v);
+    return v;
+  }
+#endif
   y1 = x1 > nx / 2 ? ny - y1 : y1;
   x1 = std::min(x1, nx - x1);
   double dx = std::min(x1, nx - x1);

@@ -13,18 +13,21 @@ import oracle
 from parity import config_from
 
 GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.json")))
-# Tolerances against the reference's printed scores (six decimals, FP32 arithmetic):
-#  * norm_type=0 without phase flip: every stage is well defined and the FP64 oracle agrees
-#    with the reference to 2e-6 relative; pinned at 2e-5.
-#  * norm_type=1: the reference normalises every rotated template by a mean and variance from
-#    compute_sum_sqr (kernels.cu:384-443), whose warp-synchronous tail has no volatile or
-#    __syncwarp (kernels.cu:423-436), so on Volta and later its sums are undefined.  The mean
-#    leaves a DC residue and the variance a per-template scale inside the per-pixel mean and
-#    sigma, so the printed z-scores carry that error (measured up to 3e-3 relative here; the
-#    oracle uses exact sums, as does the CUDA path).  Picks within the tolerance band of the
-#    threshold may appear on one side only.
-#  * norm_type=0 with phase flip: 2e-4 measured, 1e-3 allowed.
-REF_RTOL = {"nonorm_768_l256": 2e-5, "nonorm_768_l256_flip": 1e-3}
+# Tolerances against the reference's printed scores (six decimals, FP32 arithmetic), from the
+# measured agreement of the FP64 oracle with each fixture:
+#  * norm_type=0 without phase flip: every stage is well defined; 2e-6 to 5.4e-6 relative
+#    measured (windows 256, 320, 512), pinned at 2e-5.
+#  * norm_type=0 with phase flip: 2.0e-4 measured, 1e-3 allowed.
+#  * norm_type=1: median 2e-5 to 2.4e-4, maximum 4.6e-4 to 2.9e-3 measured (windows 256, 320,
+#    512), largest for picks within ~30 px of a window edge; 5e-3 allowed, and picks within the
+#    band of the threshold may appear on one side only.  The spread is not the reference's
+#    warp-synchronous reduction tails (kernels.cu:362-375, 423-436): a build of the same
+#    sources with kernels.cu compiled for device debug (picks_sync, oracle/ref_build.sh) prints
+#    the same picks with scores within 5e-7 (test below).  Emulating the reference's FP32 CTF,
+#    its FP32 sweep statistics or an FP32 template transform in the oracle leaves it unchanged
+#    as well; its source is not pinned.
+REF_RTOL = {"nonorm_768_l256": 2e-5, "nonorm_1024_l320": 2e-5, "nonorm_1024_l512_t8": 2e-5,
+            "nonorm_768_l256_flip": 1e-3}
 REF_RTOL_DEFAULT = 5e-3
 REF_ATOL = 2e-6
 
@@ -95,3 +98,20 @@ def test_gpu_matches_reference_picks(path):
     picks = s.search(img, ctf)
     missing, extra, bad = check_against_reference(g, picks, cfg.threshold)
     assert not missing and not extra and not bad, (missing[:5], extra[:5], bad[:5])
+
+
+SYNC = [p for p in GOLDEN if "picks_sync" in load(p)]
+
+
+@pytest.mark.skipif(not SYNC, reason="no fixture with the warp-safe build's picks")
+@pytest.mark.parametrize("path", SYNC, ids=[os.path.basename(p)[:-5] for p in SYNC])
+def test_warp_safe_reference_build_prints_the_same_picks(path):
+    """The reference's sources with kernels.cu built for device debug (its warp-synchronous
+    reduction tails then read what their neighbours wrote) print the same pick list, in the same
+    order, with scores within 5e-7 relative: those tails do not cause the norm_type=1 spread."""
+    g = load(path)
+    key = lambda p: (p["euler1"], p["angle"], p["x"], p["y"])
+    assert [key(p) for p in g["picks"]] == [key(p) for p in g["picks_sync"]]
+    a = np.array([p["score"] for p in g["picks"]])
+    b = np.array([p["score"] for p in g["picks_sync"]])
+    assert np.all(np.abs(a - b) <= 5e-7 * np.abs(a) + 1e-6)
