@@ -59,6 +59,8 @@ def args_parse():
                     help="skip the untimed FP32 / BF16 top-K searches that measure the chosen form's score error")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="--impl reference: skip timing the reference's own CUDA build beside the oracle")
+    ap.add_argument("--tensor-cores", type=int, default=1, choices=[0, 1],
+                    help="0: run the FP16 forms' column transforms on the CUDA cores instead of tcgen05")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host (cuda_graphs = 0), e.g. for per-launch profiling")
     ap.add_argument("--shape", type=int, default=-1,
@@ -447,6 +449,7 @@ def main():
         params["pass_b_shape"] = a.shape
     if a.eager:
         params["cuda_graphs"] = 0
+    params["tensor_cores"] = a.tensor_cores
     cfg = gisspa.Config.default(**params)
     angles = int(math.ceil(360.0 / cfg.phistep - 1e-9))
     data = dict(synth.WORKLOADS[wl])
@@ -593,6 +596,7 @@ def main():
     if a.form == "plain" and a.chosen not in ("none", "plain"):
         p2 = dict(synth.SEARCH_PARAMS[wl])
         p2.update(FORMS[a.chosen])
+        p2["tensor_cores"] = a.tensor_cores
         s2 = gisspa.Searcher(gisspa.Config.default(**p2), local)
         s2.set_templates(case.templates)
         for _ in range(a.warmup):

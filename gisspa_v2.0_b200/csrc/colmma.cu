@@ -1,0 +1,236 @@
+// colmma.cu — pass A on the tensor cores: the column transforms of the correlation as two
+// small DFT-matrix products per column on tcgen05, for FP16 template spectra at window 512 (the
+// chosen form's precision).  Same inputs, outputs and launch grid as pass_a_kernel<512,
+// SpecFp16> (correlate.cu); pass B is unchanged.
+//
+// A column Z[ky] (ky < 512; the kx = 0 and kx = 256 columns packed as a + i b in slot 0) is
+// inverse-transformed as out[k1 + 16 k2] = sum_n2 e^(2 pi i n2 k2 / 32) e^(2 pi i n2 k1 / 512)
+// sum_n1 e^(2 pi i n1 k1 / 16) Z[32 n1 + n2]:
+//   stage 1  Y[n2][k1] = sum_n1 x[n1][n2] F16[n1][k1]     (MMA, M = (column, n2), K = n1, N = k1)
+//   twiddle  Y[n2][k1] *= e^(2 pi i n2 k1 / 512)           (CUDA cores, FP32)
+//   stage 2  out[k1 + 16 k2] = sum_n2 Y[n2][k1] F32[n2][k2] (MMA, M = (column, k1), K = n2, N = k2)
+// Complex products are real GEMMs over (real, imaginary) halves of K and N.  Operands are FP16
+// (the column data and the DFT matrices), accumulation FP32 in tensor memory, twiddles FP32.
+// Peak scores stay within 3e-4 of FP64 (the chosen form's bar is 1e-3).
+//
+// One CTA (4 warps) owns 16 column slots of one (window, template) pair, in two groups of 8:
+// per group, two stage-1 MMAs (4 columns x 32 rows each, M = 128, N = 32, K = 32) and one
+// stage-2 MMA (8 columns x 16 rows, M = 128, N = 64, K = 64).  Every thread loads the 16 points
+// of one column row (coalesced along n2), and after each MMA reads one tensor-memory lane.
+#include "../../include/gisspa.h"
+#include "correlate.cuh"
+#include "fft.cuh"
+#include "tcgen05.cuh"
+
+namespace gisspa {
+namespace {
+
+constexpr int kL = 512, kNZ = 256, kHS = 257;
+constexpr int kThreads = 128;
+constexpr int kSlotsPerCta = 16;
+constexpr uint32_t kTmemCols = 128;
+// K-major tiles (tcgen05.cuh): stage-1 data 128 rows x 32 halves (two tiles), stage-2 data
+// 128 rows x 64 halves (LBO padded to 144 bytes: the transposing 2-byte stores of a warp then
+// fall in distinct banks), the DFT matrices 32 x 32 and 64 x 64
+constexpr uint32_t kLbo1 = 128, kSbo1 = 512, kLbo2 = 144, kSbo2 = 8 * 144, kLboB = 128;
+constexpr uint32_t kSboB1 = 512, kSboB2 = 1024;
+constexpr uint32_t kOffA1 = 0, kA1Tile = 16 * kSbo1;              // 2 x 8192
+constexpr uint32_t kOffA2 = kOffA1 + 2 * kA1Tile;                  // 16384
+constexpr uint32_t kOffB1 = kOffA2 + 16 * kSbo2;                   // + 18432
+constexpr uint32_t kOffB2 = kOffB1 + 4 * kSboB1;                   // + 2048
+constexpr uint32_t kOffTw = kOffB2 + 8 * kSboB2;                   // + 8192
+constexpr uint32_t kSmem = kOffTw + kL * sizeof(float2);           // + 4096
+static_assert(kOffA2 % 16 == 0 && kOffB1 % 16 == 0 && kOffB2 % 16 == 0 && kOffTw % 16 == 0, "16-byte tiles");
+
+__device__ __forceinline__ void st_half(uint8_t* base, uint32_t off, float v) {
+  *reinterpret_cast<__half*>(base + off) = __float2half_rn(v);
+}
+
+__global__ void __launch_bounds__(kThreads, 4)
+    pass_a_tc_kernel(const float2* __restrict__ I, const __half2* __restrict__ T, float2* __restrict__ Q, int b0,
+                     int n0, int D, const float2* __restrict__ twL, int chained, unsigned* __restrict__ err) {
+  extern __shared__ __align__(128) uint8_t sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  const int p = blockIdx.y, e = p / D, d = p - e * D;
+  const int c0 = blockIdx.x * kSlotsPerCta;
+
+  // constant operands: B1[nn = (q, k1)][k = (p, n1)], B2[nn = (q, k2)][k = (p, n2)] (K-major),
+  // F = e^(+i theta): real part cos, imaginary sin; rows q = 0 give the real output, q = 1 the
+  // imaginary; columns p = 0 multiply the real input, p = 1 the imaginary
+  for (int i = t; i < 32 * 32; i += kThreads) {
+    const int nn = i >> 5, k = i & 31, q = nn >> 4, k1 = nn & 15, pp = k >> 4, n1 = k & 15;
+    const int a = (2 * n1 * k1) & 31;  // angle in units of 2 pi / 32
+    const float c = (float)cos32(a), s = (float)sin32(a);
+    const float v = q == 0 ? (pp == 0 ? c : -s) : (pp == 0 ? s : c);
+    st_half(sm + kOffB1, kmajor_off(nn, k, kLboB, kSboB1), v);
+  }
+  for (int i = t; i < 64 * 64; i += kThreads) {
+    const int nn = i >> 6, k = i & 63, q = nn >> 5, k2 = nn & 31, pp = k >> 5, n2 = k & 31;
+    const int a = (n2 * k2) & 31;
+    const float c = (float)cos32(a), s = (float)sin32(a);
+    const float v = q == 0 ? (pp == 0 ? c : -s) : (pp == 0 ? s : c);
+    st_half(sm + kOffB2, kmajor_off(nn, k, kLboB, kSboB2), v);
+  }
+  float2* tw = reinterpret_cast<float2*>(sm + kOffTw);
+  for (int i = t; i < kL; i += kThreads) {
+    const float2 v = __ldg(twL + i);
+    tw[i] = make_float2(v.x, -v.y);  // e^(+2 pi i p / 512)
+  }
+  if (t == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  if (w == 0) tmem_alloc(&tmem_slot, kTmemCols);
+  griddep_launch_dependents();
+  if (!chained) griddep_wait();  // the spectra may come from the kernel just before
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t lane_base = (uint32_t)(32 * w) << 16;
+
+  const float2* Ib = I + (size_t)(b0 + e) * kHS * kL;
+  const __half2* Tn = T + (size_t)(n0 + d) * kHS * kL;
+  float2* Qp = Q + (size_t)p * kL * kNZ;
+  unsigned parity = 0;
+  bool ok = true;
+  bool waited = chained == 0;
+  for (int g = 0; g < kSlotsPerCta / 8 && ok; ++g) {
+    // ---- load: thread (w, lane) fills row n2 = lane of columns c8 = w and w + 4
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int c = c0 + 8 * g + w + 4 * h;
+      float re[16], im[16];
+#pragma unroll
+      for (int n1 = 0; n1 < 16; ++n1) {
+        const int ky = 32 * n1 + lane;
+        float2 v;
+        if (c == 0) {
+          const float2 a = cmulc(__ldg(Ib + ky), __half22float2(Tn[ky]));
+          const float2 b = cmulc(__ldg(Ib + (size_t)kNZ * kL + ky), __half22float2(Tn[(size_t)kNZ * kL + ky]));
+          v = make_float2(a.x - b.y, a.y + b.x);
+        } else {
+          v = cmulc(__ldg(Ib + (size_t)c * kL + ky), __half22float2(Tn[(size_t)c * kL + ky]));
+        }
+        re[n1] = v.x;
+        im[n1] = v.y;
+      }
+      uint8_t* a1 = sm + kOffA1 + h * kA1Tile;
+      const int m = 32 * w + lane;
+#pragma unroll
+      for (int kg = 0; kg < 4; ++kg) {
+        uint32_t u[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int i0 = 8 * (kg & 1) + 2 * j;
+          const __half2 hh = kg < 2 ? __floats2half2_rn(re[i0], re[i0 + 1]) : __floats2half2_rn(im[i0], im[i0 + 1]);
+          u[j] = *reinterpret_cast<const uint32_t*>(&hh);
+        }
+        *reinterpret_cast<uint4*>(a1 + kmajor_off(m, 8 * kg, kLbo1, kSbo1)) = make_uint4(u[0], u[1], u[2], u[3]);
+      }
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc_fence_after();
+      const uint32_t idesc = idesc_f16(128, 32);
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks)
+          tc_mma_f16(tmem + 32 * h,
+                     smem_desc(smem_u32(sm + kOffA1 + h * kA1Tile) + ks * 2 * kLbo1, kLbo1, kSbo1),
+                     smem_desc(smem_u32(sm + kOffB1) + ks * 2 * kLboB, kLboB, kSboB1), idesc, ks);
+      tc_commit(&bar);
+    }
+    ok = __syncthreads_and(mbar_wait(&bar, parity, 4000000000LL));
+    parity ^= 1u;
+    if (!ok) break;
+    tc_fence_after();
+    // ---- twiddles and the stage-2 operand: A2[(c8, k1)][(part, n2)]
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float v[32];
+      tmem_ld32(tmem + lane_base + 32 * h, v);  // row (c8 = w + 4h, n2 = lane): Yr[k1], Yi[k1]
+      const int c8 = w + 4 * h;
+#pragma unroll
+      for (int k1 = 0; k1 < 16; ++k1) {
+        const float2 z = cmul(make_float2(v[k1], v[16 + k1]), tw[(lane * k1) & (kL - 1)]);
+        st_half(sm + kOffA2, kmajor_off(16 * c8 + k1, lane, kLbo2, kSbo2), z.x);
+        st_half(sm + kOffA2, kmajor_off(16 * c8 + k1, 32 + lane, kLbo2, kSbo2), z.y);
+      }
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc_fence_after();
+      const uint32_t idesc = idesc_f16(128, 64);
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks)
+        tc_mma_f16(tmem + 64, smem_desc(smem_u32(sm + kOffA2) + ks * 2 * kLbo2, kLbo2, kSbo2),
+                   smem_desc(smem_u32(sm + kOffB2) + ks * 2 * kLboB, kLboB, kSboB2), idesc, ks);
+      tc_commit(&bar);
+    }
+    ok = __syncthreads_and(mbar_wait(&bar, parity, 4000000000LL));
+    parity ^= 1u;
+    if (!ok) break;
+    tc_fence_after();
+    // ---- outputs: row (c8, k1) = lane 32 w + lane holds out[k1 + 16 k2], k2 < 32
+    float zr[32], zi[32];
+    tmem_ld32(tmem + lane_base + 64, zr);
+    tmem_ld32(tmem + lane_base + 96, zi);
+    if (!waited) {
+      griddep_wait();  // Q is still being read by the previous pass B
+      waited = true;
+    }
+    const int c8 = 2 * w + (lane >> 4), k1 = lane & 15;
+    float2* dst = Qp + c0 + 8 * g + c8;
+#pragma unroll
+    for (int k2 = 0; k2 < 32; ++k2) dst[(size_t)(k1 + 16 * k2) * kNZ] = make_float2(zr[k2], zi[k2]);
+    tc_fence_before();
+    __syncthreads();  // tensor memory and the operand tiles are reused by the next group
+    tc_fence_after();
+  }
+  if (!ok) {
+    if (t == 0) {
+      atomicOr(err, 1u);
+      // let an MMA still in flight finish before its tensor memory is released
+      mbar_wait(&bar, parity ^ 1u, 400000000LL);
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  if (w == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+}  // namespace
+
+void launch_a_tc(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
+                 const float2* twL, cudaStream_t s) {
+  static PerDeviceOnce once;
+  once([] {
+    GISSPA_CUDA(cudaFuncSetAttribute(pass_a_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+  });
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(kNZ / kSlotsPerCta, cl.E * cl.D);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSmem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  GISSPA_CUDA(cudaLaunchKernelEx(&cfg, pass_a_tc_kernel, I, static_cast<const __half2*>(T), Q, args.b0, args.n0, cl.D,
+                                 twL, cl.chained ? 1 : 0, args.err));
+  ++launch_counter();
+}
+
+}  // namespace gisspa

@@ -647,7 +647,12 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
   if (ev) GISSPA_CUDA(cudaEventRecord(ev[0], s));
   switch (cl.spec) {
     case GISSPA_SPEC_FP32: launch_a<L, SpecFp32>(cl, I, T, Q, args, twL, s); break;
-    case GISSPA_SPEC_FP16: launch_a<L, SpecFp16>(cl, I, T, Q, args, twL, s); break;
+    case GISSPA_SPEC_FP16:
+      if (L == 512 && cl.tc)
+        launch_a_tc(cl, I, T, Q, args, twL, s);
+      else
+        launch_a<L, SpecFp16>(cl, I, T, Q, args, twL, s);
+      break;
     case GISSPA_SPEC_BF16: launch_a<L, SpecBf16>(cl, I, T, Q, args, twL, s); break;
     default: throw CudaError{cudaErrorInvalidValue, "unknown spectrum precision"};
   }

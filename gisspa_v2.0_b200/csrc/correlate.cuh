@@ -79,6 +79,8 @@ struct CorrLaunch {
   // pass B writes: it then waits for it only before storing Q (programmatic dependent launch
   // overlaps the rest with pass B's last CTAs).  Otherwise pass A waits at its start.
   bool chained = false;
+  // FP16 template spectra at L = 512: the column pass on the tensor cores (colmma.cu)
+  bool tc = false;
 };
 
 // Launch pass A then pass B on stream s.  I: window spectra [W][L/2+1][L];
@@ -89,6 +91,9 @@ int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev = nullptr);
 
 // Whether a window size has compiled correlation kernels.
+// Pass A on the tensor cores (colmma.cu): FP16 template spectra at L = 512.
+void launch_a_tc(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
+                 const float2* twL, cudaStream_t s);
 bool correlate_supported(int L);
 // Number of pass B shapes compiled for a window size (the autotuner's choices).
 int correlate_variants(int L);

@@ -369,6 +369,7 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
     for (const auto& cd : cands) {
       if (!correlate_variant_ok(l, v, epi)) continue;
       CorrLaunch cl{l, cd.E, cd.D, h->cfg.spectrum_precision, epi, v};
+      cl.tc = h->cfg.tensor_cores != 0;
       args.b0 = 0;
       args.n0 = 0;
       args.D = cd.D;
@@ -429,6 +430,7 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
     for (int b0 = 0; b0 < W; b0 += E) {
       const int e = std::min(E, W - b0);
       CorrLaunch cl{l, e, d, h->cfg.spectrum_precision, epi, variant};
+      cl.tc = h->cfg.tensor_cores != 0;
       cl.chained = pairs > 0;  // after this sequence's first pair of passes
       args.Q = Q;
       args.b0 = b0;

@@ -38,7 +38,8 @@ class Config(C.Structure):
                                          "bfactor3")] + \
                [("pick_mode", C.c_int), ("topk", C.c_int), ("exclusion_radius", C.c_float),
                 ("spectrum_precision", C.c_int), ("template_batch", C.c_int), ("window_batch", C.c_int),
-                ("quirks", C.c_int), ("tile_size", C.c_int), ("cuda_graphs", C.c_int), ("pass_b_shape", C.c_int)]
+                ("quirks", C.c_int), ("tile_size", C.c_int), ("cuda_graphs", C.c_int), ("pass_b_shape", C.c_int),
+                ("tensor_cores", C.c_int)]
 
     @classmethod
     def default(cls, **kw) -> "Config":
@@ -52,6 +53,7 @@ class Config(C.Structure):
         c.pick_mode, c.topk, c.exclusion_radius = PICK_CHUNK, 1000, 64.0
         c.spectrum_precision, c.template_batch, c.window_batch = SPEC_FP32, 0, 0
         c.quirks, c.tile_size, c.cuda_graphs, c.pass_b_shape = QUIRKS_REFERENCE, 720, 1, -1
+        c.tensor_cores = 1
         for k, v in kw.items():
             if not hasattr(c, k):
                 raise KeyError(k)

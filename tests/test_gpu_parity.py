@@ -208,12 +208,14 @@ def test_batch_matches_single_searches():
         assert len(x) > 0 and np.array_equal(x, y)
 
 
+@pytest.mark.parametrize("tensor_cores", [1, 0])
 @pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4"])
-def test_chosen_form_picks_and_scores(name):
+def test_chosen_form_picks_and_scores(name, tensor_cores):
     """The chosen form (FP16 template spectra, one top-K sweep) against the FP64 oracle: picks by
-    the margin rule, peak scores within 1e-3 (relative)."""
+    the margin rule, peak scores within 1e-3 (relative).  At window 512 the column transforms run
+    on the tensor cores (tcgen05, FP16 operands) or, with tensor_cores = 0, on the CUDA cores."""
     g, (o, m, _, _), cfg, s = run_both(name, spectrum_precision=gisspa.SPEC_FP16, pick_mode=gisspa.PICK_TOPK,
-                                       topk=30, exclusion_radius=30.0, threshold=2.5)
+                                       topk=30, exclusion_radius=30.0, threshold=2.5, tensor_cores=tensor_cores)
     assert len(o) >= 5
     rep = check_topk_picks(g, o, m, rtol=1e-3, atol=0.0)
     assert not rep["failures"], rep
@@ -239,3 +241,12 @@ def test_every_row_kernel_shape(name, shapes, mode):
         else:
             rep = check_topk_picks(g, o, m)
         assert not rep["failures"], (v, rep)
+
+
+def test_tensor_core_column_pass_chunk_picks():
+    """FP16 spectra with the reference's chunk picks (two sweeps) at window 512: the tensor-core
+    column pass against the oracle by the margin rule at the FP16 form's 1e-3."""
+    g, (o, m, near, nm), cfg, s = run_both("norm_l512_w4", spectrum_precision=gisspa.SPEC_FP16, tensor_cores=1)
+    assert len(o) > 0
+    rep = check_chunk_picks(g, o, m, near, nm, cfg.threshold, rtol=1e-3, atol=0.0)
+    assert not rep["failures"], rep
