@@ -210,7 +210,235 @@ __global__ void __launch_bounds__(kThreads, 4)
   }
 }
 
+// ---- pass B on the tensor cores (top-K epilogue)
+//
+// A row of the map (512 real pixels) comes from its half row Q[y][0..256) through the unpack
+// Z[k] = E[k] + i W_512^-k O[k] (CUDA cores) and the 256-point inverse transform
+// X[k1 + 16 k2] = sum_n2 e^(2 pi i n2 k2 / 16) e^(2 pi i n2 k1 / 256) sum_n1 e^(2 pi i n1 k1 / 16)
+// Z[16 n1 + n2], pixels (2j, 2j + 1) = (Re, Im) X[j]:
+//   stage 1  M = (row, n2) 8 x 16, K = (part, n1) 32, N = (part, k1) 32
+//   twiddle  e^(2 pi i n2 k1 / 256), FP32
+//   stage 2  M = (row, k1) 8 x 16, K = (part, n2) 32, N = (part, k2) 32
+// against one 16-point DFT matrix as a real 32 x 32 block.  A CTA (4 warps) owns 8 rows of one
+// window and loops over the launch's D templates; the rows of each template arrive by one bulk
+// copy into a double-buffered stage, as in pass B.  Thread t reads tensor-memory lane t: after
+// stage 2 that is (row t / 16, k1 = t % 16), the same 32 pixels for every template, whose sums,
+// squares and maxima stay in registers and are folded into the state once per launch.
+constexpr int kRowsB = 8;
+constexpr uint32_t kTmemColsB = 64;
+constexpr uint32_t kLboA = 128, kSboA = 512;           // stage-1 operand 128 x 32
+constexpr uint32_t kLboC = 144, kSboC = 4 * 144;       // stage-2 operand 128 x 32 (padded)
+constexpr uint32_t kStageB = kRowsB * kNZ * sizeof(float2);               // 16384 per template
+constexpr uint32_t kOffStage = 0;                                          // 2 x 16384
+constexpr uint32_t kOffOpA = 2 * kStageB;                                  // 32768, 8192
+constexpr uint32_t kOffOpC = kOffOpA + 16 * kSboA;                         // 40960, 9216
+constexpr uint32_t kOffDft = kOffOpC + 16 * kSboC;                         // 50176, 2048
+constexpr uint32_t kOffTwL = kOffDft + 4 * 512;                            // 52224, 2048
+constexpr uint32_t kOffTwN = kOffTwL + kNZ * sizeof(float2);              // 54272, 2048
+constexpr uint32_t kSmemB = kOffTwN + kNZ * sizeof(float2);               // 56320
+static_assert(kOffOpA % 128 == 0 && kOffOpC % 16 == 0 && kOffDft % 16 == 0 && kOffTwL % 16 == 0, "aligned tiles");
+
+__global__ void __launch_bounds__(kThreads, 2)
+    pass_b_tc_kernel(CorrArgs a, const float2* __restrict__ twL, const float2* __restrict__ twNZ) {
+  extern __shared__ __align__(128) uint8_t sm[];
+  __shared__ __align__(8) uint64_t bars[3];  // two stage buffers, the MMAs
+  __shared__ uint32_t tmem_slot;
+  const int t = threadIdx.x, w = t >> 5;
+  const int e = blockIdx.y, y0 = blockIdx.x * kRowsB, win = a.b0 + e;
+  const int angle = a.angle_state ? a.angle_state->index : a.angle;
+  float2* tw_l = reinterpret_cast<float2*>(sm + kOffTwL);
+  float2* tw_n = reinterpret_cast<float2*>(sm + kOffTwN);
+  for (int i = t; i < kNZ; i += kThreads) {
+    tw_l[i] = __ldg(twL + i);
+    const float2 v = __ldg(twNZ + i);
+    tw_n[i] = make_float2(v.x, -v.y);  // e^(+2 pi i p / 256)
+  }
+  // the 16-point inverse DFT as a real block: rows (q, k1), columns (p, n1), K-major
+  for (int i = t; i < 32 * 32; i += kThreads) {
+    const int nn = i >> 5, k = i & 31, q = nn >> 4, k1 = nn & 15, pp = k >> 4, n1 = k & 15;
+    const int ang = (2 * n1 * k1) & 31;
+    const float c = (float)cos32(ang), s = (float)sin32(ang);
+    st_half(sm + kOffDft, kmajor_off(nn, k, kLboB, kSboB1), q == 0 ? (pp == 0 ? c : -s) : (pp == 0 ? s : c));
+  }
+  if (t == 0) {
+    for (int i = 0; i < 3; ++i) mbar_init(&bars[i], 1);
+    fence_mbar_init();
+  }
+  if (w == 0) tmem_alloc(&tmem_slot, kTmemColsB);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t lane_base = (uint32_t)(32 * w) << 16;
+  griddep_launch_dependents();
+  griddep_wait();  // Q comes from the pass A just before
+  auto issue = [&](int d) {
+    const float2* src = a.Q + ((size_t)(e * a.D + d) * kL + y0) * kNZ;
+    fence_proxy_async_smem();
+    mbar_expect_tx(&bars[d & 1], kStageB);
+    bulk_g2s(sm + kOffStage + (d & 1) * kStageB, src, kStageB, &bars[d & 1]);
+  };
+  if (t == 0) issue(0);
+
+  // this thread's 32 pixels after stage 2: row r, pixels 2 (k1 + 16 k2) + {0, 1}
+  const int r2 = t >> 4, k1o = t & 15;
+  float acc1[32], acc2[32], best[32];
+  int barg[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    acc1[i] = 0.f;
+    acc2[i] = 0.f;
+    best[i] = -INFINITY;
+    barg[i] = -1;
+  }
+  int issued = 1, dcur = 0;
+  unsigned mma_parity = 0;
+  bool ok = true;
+  for (int d = 0; d < a.D; ++d) {
+    dcur = d;
+    if (t == 0 && d + 1 < a.D) {
+      issue(d + 1);
+      ++issued;
+    }
+    ok = __syncthreads_and(mbar_wait(&bars[d & 1], (d >> 1) & 1, 4000000000LL));
+    if (!ok) break;
+    const float2* stg = reinterpret_cast<const float2*>(sm + kOffStage + (d & 1) * kStageB);
+    // unpack: thread t fills operand row (r = t / 16, n2 = t % 16) with Z[16 n1 + n2], n1 < 16
+    {
+      const int r = t >> 4, n2 = t & 15;
+      const float2* row = stg + r * kNZ;
+      uint32_t pk_re[8], pk_im[8];
+#pragma unroll
+      for (int n1 = 0; n1 < 16; n1 += 2) {
+        const float2 z0 = row_unpack<kNZ>(row, tw_l, 16 * n1 + n2);
+        const float2 z1 = row_unpack<kNZ>(row, tw_l, 16 * (n1 + 1) + n2);
+        const __half2 hr = __floats2half2_rn(z0.x, z1.x), hi = __floats2half2_rn(z0.y, z1.y);
+        pk_re[n1 >> 1] = *reinterpret_cast<const uint32_t*>(&hr);
+        pk_im[n1 >> 1] = *reinterpret_cast<const uint32_t*>(&hi);
+      }
+      uint8_t* op = sm + kOffOpA;
+      *reinterpret_cast<uint4*>(op + kmajor_off(t, 0, kLboA, kSboA)) = make_uint4(pk_re[0], pk_re[1], pk_re[2], pk_re[3]);
+      *reinterpret_cast<uint4*>(op + kmajor_off(t, 8, kLboA, kSboA)) = make_uint4(pk_re[4], pk_re[5], pk_re[6], pk_re[7]);
+      *reinterpret_cast<uint4*>(op + kmajor_off(t, 16, kLboA, kSboA)) = make_uint4(pk_im[0], pk_im[1], pk_im[2], pk_im[3]);
+      *reinterpret_cast<uint4*>(op + kmajor_off(t, 24, kLboA, kSboA)) = make_uint4(pk_im[4], pk_im[5], pk_im[6], pk_im[7]);
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();  // the stage buffer is free again: every row was unpacked
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks)
+        tc_mma_f16(tmem, smem_desc(smem_u32(sm + kOffOpA) + ks * 2 * kLboA, kLboA, kSboA),
+                   smem_desc(smem_u32(sm + kOffDft) + ks * 2 * kLboB, kLboB, kSboB1), idesc_f16(128, 32), ks);
+      tc_commit(&bars[2]);
+    }
+    ok = __syncthreads_and(mbar_wait(&bars[2], mma_parity, 4000000000LL));
+    mma_parity ^= 1u;
+    if (!ok) break;
+    tc_fence_after();
+    {
+      float v[32];
+      tmem_ld32(tmem + lane_base, v);  // lane t = (r, n2): Y[k1] re, im
+      const int r = t >> 4, n2 = t & 15;
+#pragma unroll
+      for (int k1 = 0; k1 < 16; ++k1) {
+        const float2 z = cmul(make_float2(v[k1], v[16 + k1]), tw_n[n2 * k1]);
+        st_half(sm + kOffOpC, kmajor_off(16 * r + k1, n2, kLboC, kSboC), z.x);
+        st_half(sm + kOffOpC, kmajor_off(16 * r + k1, 16 + n2, kLboC, kSboC), z.y);
+      }
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks)
+        tc_mma_f16(tmem + 32, smem_desc(smem_u32(sm + kOffOpC) + ks * 2 * kLboC, kLboC, kSboC),
+                   smem_desc(smem_u32(sm + kOffDft) + ks * 2 * kLboB, kLboB, kSboB1), idesc_f16(128, 32), ks);
+      tc_commit(&bars[2]);
+    }
+    ok = __syncthreads_and(mbar_wait(&bars[2], mma_parity, 4000000000LL));
+    mma_parity ^= 1u;
+    if (!ok) break;
+    tc_fence_after();
+    {
+      float x[32];
+      tmem_ld32(tmem + lane_base + 32, x);  // lane t = (r, k1): X[k1 + 16 k2] re (k2 < 16), im
+      const int kk = angle * a.nt_total + a.n0 + d;
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float c = x[16 * h + k2];  // raw: the 1/L^2 is applied when folding
+          const int i = 2 * k2 + h;
+          acc1[i] += c;
+          acc2[i] = fmaf(c, c, acc2[i]);
+          if (c > best[i]) {
+            best[i] = c;
+            barg[i] = kk;
+          }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();  // operand tiles and tensor memory are reused by the next template
+    tc_fence_after();
+  }
+  if (!ok) {
+    if (t == 0) {
+      atomicOr(a.err, 1u);
+      mbar_wait(&bars[2], mma_parity ^ 1u, 400000000LL);  // an MMA that may still be in flight
+    }
+  } else {
+    const float inv = 1.0f / (float)(kL * kL);
+    const size_t wbase = (size_t)win * kL * kL;
+    const int oy = (y0 + r2 + kL / 2) & (kL - 1);
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int i = 2 * k2 + h;
+        const int ox = (2 * (k1o + 16 * k2) + h + kL / 2) & (kL - 1);
+        const size_t pix = wbase + (size_t)oy * kL + ox;
+        atomicAdd(a.S1 + pix, (double)(acc1[i] * inv));
+        atomicAdd(a.S2 + pix, (double)(acc2[i] * (inv * inv)));
+        if (barg[i] >= 0)
+          atomicMax(a.peak + pix, ((unsigned long long)float_key(best[i] * inv) << 32) |
+                                      (unsigned)(0xFFFFFFFFu - (unsigned)barg[i]));
+      }
+  }
+  // after a failed wait, let bulk copies still in flight land before the shared memory goes away
+  if (!ok && t == 0)
+    for (int k = dcur; k < issued; ++k) mbar_wait(&bars[k & 1], (k >> 1) & 1, 400000000LL);
+  tc_fence_before();
+  __syncthreads();
+  if (w == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, kTmemColsB);
+  }
+}
+
 }  // namespace
+
+void launch_b_tc(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ, cudaStream_t s) {
+  static PerDeviceOnce once;
+  once([] {
+    GISSPA_CUDA(cudaFuncSetAttribute(pass_b_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemB));
+  });
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(kL / kRowsB, cl.E);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSmemB;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  GISSPA_CUDA(cudaLaunchKernelEx(&cfg, pass_b_tc_kernel, args, twL, twNZ));
+  ++launch_counter();
+}
 
 void launch_a_tc(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                  const float2* twL, cudaStream_t s) {

@@ -148,24 +148,6 @@ __device__ __forceinline__ bool team_any(bool pred) {
 // of Z[k] = E[k] + i W_L^-k O[k] (E, O: the even / odd parts of the half row) and lane output j
 // = (x[2j], x[2j + 1]).  EIN inputs and EOUT outputs per lane; the row's shared-memory slice is
 // the exchange buffer once every lane of the team has read its inputs.
-template <int NZ>
-__device__ __forceinline__ float2 row_unpack(const float2* row, const float2* tw_l, int k) {
-  float2 xk, xm;
-  if (k == 0) {
-    const float2 q = row[0];
-    xk = make_float2(q.x, 0.f);
-    xm = make_float2(q.y, 0.f);
-  } else {
-    xk = row[k];
-    xm = row[NZ - k];
-  }
-  const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
-  const float2 od = make_float2(xk.x - xm.x, xk.y + xm.y);
-  float2 w = tw_l[k];
-  w.y = -w.y;
-  const float2 o = cmul(w, od);
-  return make_float2(ev.x - o.y, ev.y + o.x);
-}
 template <int L, int TEAM>
 struct RowXform {
   static constexpr int NZ = L / 2, EIN = NZ / TEAM, EOUT = NZ / TEAM, EBUF = EIN;
@@ -658,6 +640,11 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
   }
   if (ev) GISSPA_CUDA(cudaEventRecord(ev[1], s));
   if constexpr (L == 512) {
+    if (cl.tc && cl.spec == GISSPA_SPEC_FP16 && cl.epi == EPI_TOPK) {
+      launch_b_tc(cl, args, twL, twNZ, s);
+      if (ev) GISSPA_CUDA(cudaEventRecord(ev[2], s));
+      return 2;
+    }
     switch (cl.variant) {
       case 1: launch_b<L, 1>(cl, args, twL, twNZ, s); break;
       case 2: launch_b<L, 2>(cl, args, twL, twNZ, s); break;

@@ -91,9 +91,33 @@ int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev = nullptr);
 
 // Whether a window size has compiled correlation kernels.
+// One input of a row's half-length inverse transform: from the row's Hermitian half (slot 0
+// packing the kx = 0 and kx = L/2 terms as its real and imaginary parts), Z[k] = E[k] +
+// i W_L^-k O[k] with E, O the even and odd parts (tw_l: e^(-2 pi i k / L), k < NZ).
+template <int NZ>
+__device__ __forceinline__ float2 row_unpack(const float2* row, const float2* tw_l, int k) {
+  float2 xk, xm;
+  if (k == 0) {
+    const float2 q = row[0];
+    xk = make_float2(q.x, 0.f);
+    xm = make_float2(q.y, 0.f);
+  } else {
+    xk = row[k];
+    xm = row[NZ - k];
+  }
+  const float2 ev = make_float2(xk.x + xm.x, xk.y - xm.y);
+  const float2 od = make_float2(xk.x - xm.x, xk.y + xm.y);
+  float2 w = tw_l[k];
+  w.y = -w.y;
+  const float2 o = cmul(w, od);
+  return make_float2(ev.x - o.y, ev.y + o.x);
+}
+
 // Pass A on the tensor cores (colmma.cu): FP16 template spectra at L = 512.
 void launch_a_tc(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                  const float2* twL, cudaStream_t s);
+// Pass B on the tensor cores with the top-K epilogue (colmma.cu): FP16 template spectra at L = 512.
+void launch_b_tc(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ, cudaStream_t s);
 bool correlate_supported(int L);
 // Number of pass B shapes compiled for a window size (the autotuner's choices).
 int correlate_variants(int L);

@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <future>
 #include <sstream>
 #include <string>
 #include <thread>
@@ -130,11 +131,27 @@ int run_device(int dev, const gisspa_config& cfg, const TemplateSource& ts, int 
                  : gisspa_set_templates(h, ts.data.data(), nt, ts.tw, ts.th);
   if (st) std::fprintf(stderr, "device %d: %s\n", dev, gisspa_last_error(h));
   std::vector<gisspa_pick> picks(1 << 16);
+  // Read-ahead: micrograph i + 1 is read and decoded on a host thread while micrograph i is
+  // searched on the GPU.
+  struct Mic {
+    bool ok = false;
+    std::vector<float> img;
+    int nx = 0, ny = 0, nz = 0;
+  };
+  auto read_one = [&lst](int i) {
+    Mic m;
+    m.ok = read_mrc(lst[i].rpath, lst[i].unused, m.img, m.nx, m.ny, m.nz);
+    return m;
+  };
+  std::future<Mic> next;
+  if (first < last && !st) next = std::async(std::launch::async, read_one, first);
   for (int i = first; i < last && !st; ++i) {
     const LstEntry& e = lst[i];
-    std::vector<float> img;
-    int nx, ny, nz;
-    if (!read_mrc(e.rpath, e.unused, img, nx, ny, nz)) {
+    Mic cur = next.get();
+    if (i + 1 < last) next = std::async(std::launch::async, read_one, i + 1);
+    std::vector<float>& img = cur.img;
+    const int nx = cur.nx, ny = cur.ny;
+    if (!cur.ok) {
       std::fprintf(stderr, "cannot read micrograph %s\n", e.rpath.c_str());
       st = GISSPA_ERR_IO;
       break;

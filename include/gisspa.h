@@ -82,8 +82,9 @@ typedef struct gisspa_config {
   int pass_b_shape;       /* with template_batch and window_batch set: row-transform kernel shape
                              (0.. compiled shapes - 1; -1 = the first); ignored when autotuning */
   int tensor_cores;       /* 1 (default): with FP16 template spectra at window_size 512 the column
-                             transforms of the correlation run on the tensor cores (tcgen05);
-                             0: on the CUDA cores, as every other form */
+                             transforms of the correlation, and with top-K picking also the row
+                             transforms, run on the tensor cores (tcgen05, FP16 operands, FP32
+                             accumulation); 0: on the CUDA cores, as every other form */
 } gisspa_config;
 
 /* Per-micrograph CTF, as in an LST line "defocus= dfdiff= dfang=" (DataReader2.h:93-103).
