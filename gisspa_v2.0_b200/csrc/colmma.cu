@@ -27,7 +27,7 @@ namespace {
 
 constexpr int kL = 512, kNZ = 256, kHS = 257;
 constexpr int kThreads = 128;
-constexpr int kSlotsPerCta = 16;
+constexpr int kSlotsPerCta = 64;
 constexpr uint32_t kTmemCols = 128;
 // K-major tiles (tcgen05.cuh): stage-1 data 128 rows x 32 halves (two tiles), stage-2 data
 // 128 rows x 64 halves (LBO padded to 144 bytes: the transposing 2-byte stores of a warp then
@@ -38,12 +38,46 @@ constexpr uint32_t kOffA1 = 0, kA1Tile = 16 * kSbo1;              // 2 x 8192
 constexpr uint32_t kOffA2 = kOffA1 + 2 * kA1Tile;                  // 16384
 constexpr uint32_t kOffB1 = kOffA2 + 16 * kSbo2;                   // + 18432
 constexpr uint32_t kOffB2 = kOffB1 + 4 * kSboB1;                   // + 2048
-constexpr uint32_t kOffTw = kOffB2 + 8 * kSboB2;                   // + 8192
-constexpr uint32_t kSmem = kOffTw + kL * sizeof(float2);           // + 4096
-static_assert(kOffA2 % 16 == 0 && kOffB1 % 16 == 0 && kOffB2 % 16 == 0 && kOffTw % 16 == 0, "16-byte tiles");
+constexpr uint32_t kSmem = kOffB2 + 8 * kSboB2;                    // + 8192
+static_assert(kOffA2 % 16 == 0 && kOffB1 % 16 == 0 && kOffB2 % 16 == 0, "16-byte tiles");
 
 __device__ __forceinline__ void st_half(uint8_t* base, uint32_t off, float v) {
   *reinterpret_cast<__half*>(base + off) = __float2half_rn(v);
+}
+
+// The constant operands, built once per device by tc_tables_kernel and copied into every CTA's
+// shared memory: the 16-point inverse DFT as a real 32 x 32 block (rows (q, k1), columns
+// (p, n1)), the 32-point one as a real 64 x 64 block, both K-major FP16 tiles, and the FP32
+// twiddles e^(+2 pi i p / 512).  F = e^(+i theta): rows q = 0 give the real output, q = 1 the
+// imaginary; columns p = 0 multiply the real input, p = 1 the imaginary.
+constexpr uint32_t kTabB16 = 0, kTabB32 = 32 * 64, kTabTw = kTabB32 + 64 * 128, kTabBytes = kTabTw + kL * 8;
+static __device__ __align__(16) uint8_t g_tc_tables[kTabBytes];
+
+__global__ void tc_tables_kernel() {
+  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
+    const int nn = i >> 5, k = i & 31, q = nn >> 4, k1 = nn & 15, pp = k >> 4, n1 = k & 15;
+    const int a = (2 * n1 * k1) & 31;  // angle in units of 2 pi / 32
+    const float c = (float)cos32(a), s = (float)sin32(a);
+    st_half(g_tc_tables + kTabB16, kmajor_off(nn, k, 128, 512), q == 0 ? (pp == 0 ? c : -s) : (pp == 0 ? s : c));
+  }
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
+    const int nn = i >> 6, k = i & 63, q = nn >> 5, k2 = nn & 31, pp = k >> 5, n2 = k & 31;
+    const int a = (n2 * k2) & 31;
+    const float c = (float)cos32(a), s = (float)sin32(a);
+    st_half(g_tc_tables + kTabB32, kmajor_off(nn, k, 128, 1024), q == 0 ? (pp == 0 ? c : -s) : (pp == 0 ? s : c));
+  }
+  float2* tw = reinterpret_cast<float2*>(g_tc_tables + kTabTw);
+  for (int i = threadIdx.x; i < kL; i += blockDim.x) {
+    double sn, cs;
+    sincospi(2.0 * i / kL, &sn, &cs);
+    tw[i] = make_float2((float)cs, (float)sn);
+  }
+}
+
+// Copies n bytes (a multiple of 16) of the constant tables into shared memory.
+__device__ __forceinline__ void copy_table(uint8_t* dst, uint32_t src_off, uint32_t n) {
+  const uint4* src = reinterpret_cast<const uint4*>(g_tc_tables + src_off);
+  for (uint32_t i = threadIdx.x; i < n / 16; i += blockDim.x) reinterpret_cast<uint4*>(dst)[i] = src[i];
 }
 
 __global__ void __launch_bounds__(kThreads, 4)
@@ -56,27 +90,15 @@ __global__ void __launch_bounds__(kThreads, 4)
   const int p = blockIdx.y, e = p / D, d = p - e * D;
   const int c0 = blockIdx.x * kSlotsPerCta;
 
-  // constant operands: B1[nn = (q, k1)][k = (p, n1)], B2[nn = (q, k2)][k = (p, n2)] (K-major),
-  // F = e^(+i theta): real part cos, imaginary sin; rows q = 0 give the real output, q = 1 the
-  // imaginary; columns p = 0 multiply the real input, p = 1 the imaginary
-  for (int i = t; i < 32 * 32; i += kThreads) {
-    const int nn = i >> 5, k = i & 31, q = nn >> 4, k1 = nn & 15, pp = k >> 4, n1 = k & 15;
-    const int a = (2 * n1 * k1) & 31;  // angle in units of 2 pi / 32
-    const float c = (float)cos32(a), s = (float)sin32(a);
-    const float v = q == 0 ? (pp == 0 ? c : -s) : (pp == 0 ? s : c);
-    st_half(sm + kOffB1, kmajor_off(nn, k, kLboB, kSboB1), v);
-  }
-  for (int i = t; i < 64 * 64; i += kThreads) {
-    const int nn = i >> 6, k = i & 63, q = nn >> 5, k2 = nn & 31, pp = k >> 5, n2 = k & 31;
-    const int a = (n2 * k2) & 31;
-    const float c = (float)cos32(a), s = (float)sin32(a);
-    const float v = q == 0 ? (pp == 0 ? c : -s) : (pp == 0 ? s : c);
-    st_half(sm + kOffB2, kmajor_off(nn, k, kLboB, kSboB2), v);
-  }
-  float2* tw = reinterpret_cast<float2*>(sm + kOffTw);
-  for (int i = t; i < kL; i += kThreads) {
-    const float2 v = __ldg(twL + i);
-    tw[i] = make_float2(v.x, -v.y);  // e^(+2 pi i p / 512)
+  // constant operands (g_tc_tables): B1[nn = (q, k1)][k = (p, n1)], B2[nn = (q, k2)][k = (p, n2)]
+  copy_table(sm + kOffB1, kTabB16, 2048);
+  copy_table(sm + kOffB2, kTabB32, 8192);
+  // this thread's twiddles e^(2 pi i n2 k1 / 512), n2 = lane, for every group
+  float2 twr[16];
+  {
+    const float2* tg = reinterpret_cast<const float2*>(g_tc_tables + kTabTw);
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) twr[k1] = tg[lane * k1];
   }
   if (t == 0) {
     mbar_init(&bar, 1);
@@ -158,7 +180,7 @@ __global__ void __launch_bounds__(kThreads, 4)
       const int c8 = w + 4 * h;
 #pragma unroll
       for (int k1 = 0; k1 < 16; ++k1) {
-        const float2 z = cmul(make_float2(v[k1], v[16 + k1]), tw[(lane * k1) & (kL - 1)]);
+        const float2 z = cmul(make_float2(v[k1], v[16 + k1]), twr[k1]);
         st_half(sm + kOffA2, kmajor_off(16 * c8 + k1, lane, kLbo2, kSbo2), z.x);
         st_half(sm + kOffA2, kmajor_off(16 * c8 + k1, 32 + lane, kLbo2, kSbo2), z.y);
       }
@@ -253,13 +275,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float2 v = __ldg(twNZ + i);
     tw_n[i] = make_float2(v.x, -v.y);  // e^(+2 pi i p / 256)
   }
-  // the 16-point inverse DFT as a real block: rows (q, k1), columns (p, n1), K-major
-  for (int i = t; i < 32 * 32; i += kThreads) {
-    const int nn = i >> 5, k = i & 31, q = nn >> 4, k1 = nn & 15, pp = k >> 4, n1 = k & 15;
-    const int ang = (2 * n1 * k1) & 31;
-    const float c = (float)cos32(ang), s = (float)sin32(ang);
-    st_half(sm + kOffDft, kmajor_off(nn, k, kLboB, kSboB1), q == 0 ? (pp == 0 ? c : -s) : (pp == 0 ? s : c));
-  }
+  copy_table(sm + kOffDft, kTabB16, 2048);  // the 16-point inverse DFT as a real 32 x 32 block
   if (t == 0) {
     for (int i = 0; i < 3; ++i) mbar_init(&bars[i], 1);
     fence_mbar_init();
@@ -419,12 +435,21 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 }
 
+// Builds the constant tables on the current device (idempotent; ordered before the first
+// tensor-core pass by the stream).
+void tc_tables(cudaStream_t s) {
+  tc_tables_kernel<<<1, 256, 0, s>>>();
+  GISSPA_LAUNCH_CHECK();
+}
+
 }  // namespace
 
 void launch_b_tc(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, const float2* twNZ, cudaStream_t s) {
   static PerDeviceOnce once;
-  once([] {
+  once([s] {
     GISSPA_CUDA(cudaFuncSetAttribute(pass_b_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemB));
+    GISSPA_CUDA(cudaFuncSetAttribute(pass_b_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    tc_tables(s);
   });
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(kL / kRowsB, cl.E);
@@ -443,8 +468,10 @@ void launch_b_tc(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, 
 void launch_a_tc(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                  const float2* twL, cudaStream_t s) {
   static PerDeviceOnce once;
-  once([] {
+  once([s] {
     GISSPA_CUDA(cudaFuncSetAttribute(pass_a_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+    GISSPA_CUDA(cudaFuncSetAttribute(pass_a_tc_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    tc_tables(s);
   });
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(kNZ / kSlotsPerCta, cl.E * cl.D);

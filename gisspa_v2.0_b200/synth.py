@@ -156,6 +156,11 @@ WORKLOADS = {
     # 24 templates, 4 angles
     "whole_2048_t24": dict(shape=(2048, 2048), n_particles=40, snr=0.05, n_templates=24, tsize=180, seed=3,
                            defocus=1.7, dfdiff=0.1, dfang=30.0),
+    # the reference's default window 320 on the 4096^2 micrograph with 400 templates: the
+    # reference reads past its template stack when windows (400 here) outnumber the templates
+    # (norm.cu:141-147), so its CUDA build is timed on this variant
+    "whole_4096_t400_w320": dict(shape=(4096, 4096), n_particles=300, snr=0.05, n_templates=400, tsize=180, seed=2,
+                                 defocus=1.7, dfdiff=0.1, dfang=30.0),
     # profiling case at the reference's default window size 320 (overlap 120)
     "whole_2048_t24_w320": dict(shape=(2048, 2048), n_particles=40, snr=0.05, n_templates=24, tsize=180, seed=3,
                                 defocus=1.7, dfdiff=0.1, dfang=30.0),
@@ -175,6 +180,8 @@ SEARCH_PARAMS = {
                      diameter=150.0, threshold=7.0, window_size=512, overlap=200, norm_type=1),
     "whole_2048_t24": dict(angpix=1.0, phistep=90.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                            diameter=140.0, threshold=7.0, window_size=512, overlap=192, norm_type=1),
+    "whole_4096_t400_w320": dict(angpix=1.0, phistep=5.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
+                                 diameter=140.0, threshold=7.0, window_size=320, overlap=120, norm_type=1),
     "whole_2048_t24_w320": dict(angpix=1.0, phistep=90.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0, lowres=200.0,
                                 diameter=140.0, threshold=7.0, window_size=320, overlap=120, norm_type=1),
 }
