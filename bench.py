@@ -59,8 +59,8 @@ def args_parse():
                     help="skip the untimed FP32 / BF16 top-K searches that measure the chosen form's score error")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="--impl reference: skip timing the reference's own CUDA build beside the oracle")
-    ap.add_argument("--tensor-cores", type=int, default=1, choices=[0, 1],
-                    help="0: run the FP16 forms' column transforms on the CUDA cores instead of tcgen05")
+    ap.add_argument("--tensor-cores", type=int, default=0, choices=[0, 1],
+                    help="1: run the FP16 forms' transforms on the tensor cores (tcgen05) instead of the CUDA cores")
     ap.add_argument("--eager", action="store_true",
                     help="launch every kernel from the host (cuda_graphs = 0), e.g. for per-launch profiling")
     ap.add_argument("--shape", type=int, default=-1,

@@ -52,7 +52,7 @@ void gisspa_config_default(gisspa_config* c) {
   c->quirks = GISSPA_QUIRKS_REFERENCE; c->tile_size = 720;
   c->cuda_graphs = 1;
   c->pass_b_shape = -1;
-  c->tensor_cores = 1;
+  c->tensor_cores = 0;
 }
 
 int gisspa_create(const gisspa_config* cfg, int device, gisspa_handle** out) {

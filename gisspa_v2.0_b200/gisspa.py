@@ -53,7 +53,7 @@ class Config(C.Structure):
         c.pick_mode, c.topk, c.exclusion_radius = PICK_CHUNK, 1000, 64.0
         c.spectrum_precision, c.template_batch, c.window_batch = SPEC_FP32, 0, 0
         c.quirks, c.tile_size, c.cuda_graphs, c.pass_b_shape = QUIRKS_REFERENCE, 720, 1, -1
-        c.tensor_cores = 1
+        c.tensor_cores = 0
         for k, v in kw.items():
             if not hasattr(c, k):
                 raise KeyError(k)
