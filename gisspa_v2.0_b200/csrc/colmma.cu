@@ -209,10 +209,23 @@ __global__ void __launch_bounds__(kThreads, 4)
       griddep_wait();  // Q is still being read by the previous pass B
       waited = true;
     }
+    // through a shared tile (the operand tiles are free now): rows y, 8 slots XOR-swizzled by
+    // y mod 8, read back as 16-byte slot pairs so that each row segment leaves contiguous
     const int c8 = 2 * w + (lane >> 4), k1 = lane & 15;
-    float2* dst = Qp + c0 + 8 * g + c8;
+    float2* tile = reinterpret_cast<float2*>(sm + kOffA1);
 #pragma unroll
-    for (int k2 = 0; k2 < 32; ++k2) dst[(size_t)(k1 + 16 * k2) * kNZ] = make_float2(zr[k2], zi[k2]);
+    for (int k2 = 0; k2 < 32; ++k2) {
+      const int y = k1 + 16 * k2;
+      tile[y * 8 + (c8 ^ (y & 7))] = make_float2(zr[k2], zi[k2]);
+    }
+    __syncthreads();
+    float2* dst = Qp + c0 + 8 * g;
+#pragma unroll
+    for (int i = 0; i < kL * 4 / kThreads; ++i) {
+      const int u = t + kThreads * i, y = u >> 2, k = (u & 3) * 2, sw = y & 7;
+      const float4 q = *reinterpret_cast<const float4*>(tile + y * 8 + ((k ^ sw) & ~1));
+      *reinterpret_cast<float4*>(dst + (size_t)y * kNZ + k) = (sw & 1) ? make_float4(q.z, q.w, q.x, q.y) : q;
+    }
     tc_fence_before();
     __syncthreads();  // tensor memory and the operand tiles are reused by the next group
     tc_fence_after();
@@ -249,10 +262,16 @@ __global__ void __launch_bounds__(kThreads, 4)
 constexpr int kRowsB = 8;
 constexpr uint32_t kTmemColsB = 64;
 constexpr uint32_t kLboA = 128, kSboA = 512;           // stage-1 operand 128 x 32
-constexpr uint32_t kLboC = 144, kSboC = 4 * 144;       // stage-2 operand 128 x 32 (padded)
-constexpr uint32_t kStageB = kRowsB * kNZ * sizeof(float2);               // 16384 per template
+// stage-2 operand 128 x 32: LBO 144 and SBO 592 bytes keep the transposing 2-byte stores of a
+// warp (two rows 16 apart, 16 lanes each) in distinct banks
+constexpr uint32_t kLboC = 144, kSboC = 592;
+// stage rows padded by 16 bytes (one bulk copy per row): the unpack's reads of two rows by one
+// warp then fall in distinct banks
+constexpr uint32_t kRowPitch = kNZ * sizeof(float2) + 16;                  // 2064
+constexpr uint32_t kStageB = kRowsB * kRowPitch;                           // 16512 per template
+constexpr uint32_t kStageBytes = kRowsB * kNZ * sizeof(float2);            // 16384 copied
 constexpr uint32_t kOffStage = 0;                                          // 2 x 16384
-constexpr uint32_t kOffOpA = 2 * kStageB;                                  // 32768, 8192
+constexpr uint32_t kOffOpA = 2 * kStageB + 128 - (2 * kStageB) % 128;       // 128-aligned, 8192
 constexpr uint32_t kOffOpC = kOffOpA + 16 * kSboA;                         // 40960, 9216
 constexpr uint32_t kOffDft = kOffOpC + 16 * kSboC;                         // 50176, 2048
 constexpr uint32_t kOffTwL = kOffDft + 4 * 512;                            // 52224, 2048
@@ -291,8 +310,11 @@ __global__ void __launch_bounds__(kThreads, 2)
   auto issue = [&](int d) {
     const float2* src = a.Q + ((size_t)(e * a.D + d) * kL + y0) * kNZ;
     fence_proxy_async_smem();
-    mbar_expect_tx(&bars[d & 1], kStageB);
-    bulk_g2s(sm + kOffStage + (d & 1) * kStageB, src, kStageB, &bars[d & 1]);
+    mbar_expect_tx(&bars[d & 1], kStageBytes);
+#pragma unroll
+    for (int r = 0; r < kRowsB; ++r)
+      bulk_g2s(sm + kOffStage + (d & 1) * kStageB + r * kRowPitch, src + (size_t)r * kNZ, kNZ * sizeof(float2),
+               &bars[d & 1]);
   };
   if (t == 0) issue(0);
 
@@ -322,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     // unpack: thread t fills operand row (r = t / 16, n2 = t % 16) with Z[16 n1 + n2], n1 < 16
     {
       const int r = t >> 4, n2 = t & 15;
-      const float2* row = stg + r * kNZ;
+      const float2* row = reinterpret_cast<const float2*>(reinterpret_cast<const uint8_t*>(stg) + r * kRowPitch);
       uint32_t pk_re[8], pk_im[8];
 #pragma unroll
       for (int n1 = 0; n1 < 16; n1 += 2) {
