@@ -84,7 +84,7 @@ typedef struct gisspa_config {
   int tensor_cores;       /* 1: with FP16 template spectra at window_size 512 the column transforms
                              of the correlation, and with top-K picking also the row transforms,
                              run on the tensor cores (tcgen05, FP16 operands, FP32 accumulation;
-                             same picks, scores within 1.1e-4 of the FP32 form) -- measured 2.3x
+                             same picks, scores within 1.1e-4 of the FP32 form) -- measured 1.7x
                              slower per launch pair than 0 on B200; 0 (default): CUDA cores */
 } gisspa_config;
 

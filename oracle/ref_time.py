@@ -74,15 +74,17 @@ def run(binary: str, config: str, cwd: str, timeout: float) -> float:
     return el
 
 
-def time_binaries(wl: str, binaries: dict, timeout: float = 900.0) -> dict:
-    """Per-micrograph and set-up wall time of each binary ({name: path}) on the workload's files."""
+def time_binaries(wl: str, binaries: dict, timeout: float = 900.0, single: bool = False) -> dict:
+    """Per-micrograph and set-up wall time of each binary ({name: path}) on the workload's files
+    (single: one run on a one-micrograph list, whose time includes the set-up)."""
     res = {"workload": wl, "params": synth.SEARCH_PARAMS[wl],
-           "timing": "wall clock of the whole process; per_micrograph = t(2 micrographs) - t(1)"}
+           "timing": ("wall clock of the whole process on one micrograph (set-up included)" if single else
+                      "wall clock of the whole process; per_micrograph = t(2 micrographs) - t(1)")}
     with tempfile.TemporaryDirectory() as d:
         lst1, lst2 = write_inputs(d, wl)
         for name, binary in binaries.items():
             t = {}
-            for n, lst in ((1, lst1), (2, lst2)):
+            for n, lst in ((1, lst1),) + (() if single else ((2, lst2),)):
                 cfg = os.path.join(d, f"config_{name}_{n}")
                 out = os.path.join(d, f"picks_{name}_{n}.txt")
                 write_config(cfg, wl, d, lst, n, out)
@@ -90,11 +92,13 @@ def time_binaries(wl: str, binaries: dict, timeout: float = 900.0) -> dict:
                 if n == 1:
                     with open(out) as fh:
                         res[f"{name}_picks"] = sum(1 for ln in fh if ln.strip())
-            res[name] = {"s_1_micrograph": t[1], "s_2_micrographs": t[2], "s_per_micrograph": t[2] - t[1],
-                         "s_setup": 2 * t[1] - t[2]}
+            res[name] = ({"s_1_micrograph": t[1]} if single else
+                         {"s_1_micrograph": t[1], "s_2_micrographs": t[2], "s_per_micrograph": t[2] - t[1],
+                          "s_setup": 2 * t[1] - t[2]})
             print(json.dumps({name: res[name]}), file=sys.stderr, flush=True)
     if "reference" in res and "ours" in res:
-        res["speedup_per_micrograph"] = res["reference"]["s_per_micrograph"] / res["ours"]["s_per_micrograph"]
+        k = "s_1_micrograph" if single else "s_per_micrograph"
+        res["speedup_per_micrograph"] = res["reference"][k] / res["ours"][k]
     return res
 
 
@@ -104,8 +108,9 @@ def main():
     ap.add_argument("--ref", default=os.path.join(HERE, "_ref", "gisspa_ref"))
     ap.add_argument("--ours", default=os.path.join(REPO, "gisspa_v2.0_b200", "_build", "gisspa_main"))
     ap.add_argument("--timeout", type=float, default=900.0)
+    ap.add_argument("--single", action="store_true", help="one run on one micrograph (set-up included)")
     a = ap.parse_args()
-    print(json.dumps(time_binaries(a.workload, {"reference": a.ref, "ours": a.ours}, a.timeout)))
+    print(json.dumps(time_binaries(a.workload, {"reference": a.ref, "ours": a.ours}, a.timeout, a.single)))
 
 
 if __name__ == "__main__":
