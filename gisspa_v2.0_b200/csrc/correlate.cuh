@@ -90,6 +90,27 @@ struct CorrLaunch {
 int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev = nullptr);
 
+// The pair engine (pair_engine.cu): one launch runs pass A of one batch and pass B of the batch
+// before it, so that the load-bound and the issue-bound pass share the SMs.  Window 512, epilogues
+// EPI_SUM, EPI_TOPK and EPI_CHUNK.
+struct EngineBatch {
+  int valid;          // 0: no such pass in this launch
+  int b0, n0, d, e;   // first window, first template, templates, windows
+  float2* Q;          // the batch's Q slot, row-major [d * e pairs][L][L/2]
+};
+bool engine_supported(int L, int epi);
+// Counters one engine launch uses (zeroed before the launch sequence).
+size_t engine_counter_ints();
+// b_args: the epilogue's arguments (its Q, b0, n0 and D are taken from B).  chained: the launch
+// before on the stream belongs to the same sequence (and its pass B reads the Q slot that this
+// launch's pass A writes).
+void engine_launch(int spec, int epi, const float2* I, const void* T, const EngineBatch& A, const EngineBatch& B,
+                   const CorrArgs& b_args, int* ctr, bool chained, const float2* twL, const float2* twNZ,
+                   cudaStream_t s);
+
+// The pass B shape index that selects the pair engine at window size L (-1: none).
+int engine_variant(int L);
+
 // Whether a window size has compiled correlation kernels.
 // One input of a row's half-length inverse transform: from the row's Hermitian half (slot 0
 // packing the kx = 0 and kx = L/2 terms as its real and imaginary parts), Z[k] = E[k] +

@@ -320,6 +320,45 @@ void choose_batches(const gisspa_config& cfg, int l, int W, int nt, int& D, int&
   D = std::max(1, std::min(D, nt));
 }
 
+// The pair engine's launch sequence over `batches` (first window, first template, windows,
+// templates): launch j runs pass A of batch j and pass B of batch j - 1, the batches' Q
+// alternating between the two halves of the Q buffer.  Returns the number of launches.
+struct Batch {
+  int b0, n0, e, d;
+};
+int engine_sequence(Ctx& c, int epi, const float2* I, const void* T, const std::vector<Batch>& batches, int D, int E,
+                    CorrArgs args) {
+  gisspa_handle* h = c.h;
+  const int l = c.l, nb = (int)batches.size();
+  const size_t pairs_max = (size_t)D * E;
+  float2* Q = buf<float2>(h->Q, 2 * pairs_max * (l / 2) * l);
+  const size_t stride = engine_counter_ints();
+  int* ctr = buf<int>(h->engine_ctr, (size_t)(nb + 1) * stride);
+  GISSPA_CUDA(cudaMemsetAsync(ctr, 0, (size_t)(nb + 1) * stride * sizeof(int), c.s));
+  const float2* twL = h->fft.twiddles(l);
+  const float2* twNZ = h->fft.twiddles(l / 2);
+  args.err = h->dev_err.as<unsigned>();
+  for (int j = 0; j <= nb; ++j) {
+    EngineBatch A{}, B{};
+    if (j < nb) {
+      const Batch& b = batches[j];
+      A = EngineBatch{1, b.b0, b.n0, b.d, b.e, Q + (size_t)(j & 1) * pairs_max * (l / 2) * l};
+    }
+    if (j > 0) {
+      const Batch& b = batches[j - 1];
+      B = EngineBatch{1, b.b0, b.n0, b.d, b.e, Q + (size_t)((j - 1) & 1) * pairs_max * (l / 2) * l};
+    }
+    engine_launch(h->cfg.spectrum_precision, epi, I, T, A, B, args, ctr + (size_t)j * stride, j > 0, twL, twNZ, c.s);
+  }
+  return nb + 1;
+}
+
+// Whether a search runs the pair engine when its shape is chosen (the tensor-core passes are
+// per-pass kernels).
+bool engine_ok(const gisspa_config& cfg, int l, int epi) {
+  return engine_supported(l, epi) && !(cfg.tensor_cores && cfg.spectrum_precision == GISSPA_SPEC_FP16);
+}
+
 // Autotuner: times every candidate launch shape (pass B variant, template batch D, window
 // batch E) on the sweep's own spectra, with the epilogue's outputs redirected to scratch,
 // and keeps the fastest per (window size, epilogue, precision).
@@ -359,7 +398,8 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   args.cand = nullptr;
   args.nt_total = nt;
   args.err = h->dev_err.as<unsigned>();
-  float2* Q = buf<float2>(h->Q, (size_t)maxDE * (l / 2) * l);
+  // (twice the largest batch: the pair engine alternates two Q slots)
+  float2* Q = buf<float2>(h->Q, 2 * (size_t)maxDE * (l / 2) * l);
   args.Q = Q;
   const float2* twL = h->fft.twiddles(l);
   const float2* twNZ = h->fft.twiddles(l / 2);
@@ -367,6 +407,23 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   best.us_per_pair = 1e30;
   for (int v = 0; v < correlate_variants(l); ++v)
     for (const auto& cd : cands) {
+      if (v == engine_variant(l)) {
+        if (!engine_ok(h->cfg, l, epi)) continue;
+        // the engine runs whole sequences: kReps batches (kReps + 1 launches) of the same pairs
+        constexpr int kReps = 4;
+        const std::vector<Batch> seq(kReps, Batch{0, 0, cd.E, cd.D});
+        args.Q = nullptr;
+        engine_sequence(c, epi, I, T, std::vector<Batch>(1, Batch{0, 0, cd.E, cd.D}), cd.D, cd.E, args);
+        GISSPA_CUDA(cudaEventRecord(h->ev[5], c.s));
+        engine_sequence(c, epi, I, T, seq, cd.D, cd.E, args);
+        GISSPA_CUDA(cudaEventRecord(h->ev[6], c.s));
+        GISSPA_CUDA(cudaEventSynchronize(h->ev[6]));
+        float ms = 0;
+        GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
+        const double us = 1000.0 * ms / (kReps * cd.D * cd.E);
+        if (us < best.us_per_pair) best = TuneChoice{v, cd.D, cd.E, us};
+        continue;
+      }
       if (!correlate_variant_ok(l, v, epi)) continue;
       CorrLaunch cl{l, cd.E, cd.D, h->cfg.spectrum_precision, epi, v};
       cl.tc = h->cfg.tensor_cores != 0;
@@ -394,7 +451,8 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
   int variant = 0;
   const bool generic = !correlate_fast(l);  // no hand-tuned kernels for this window size
   if (!generic && h->cfg.template_batch > 0 && h->cfg.window_batch > 0 && h->cfg.pass_b_shape >= 0) {
-    if (!correlate_variant_ok(l, h->cfg.pass_b_shape, epi))
+    if (!correlate_variant_ok(l, h->cfg.pass_b_shape, epi) ||
+        (h->cfg.pass_b_shape == engine_variant(l) && !engine_ok(h->cfg, l, epi)))
       throw CudaError{cudaErrorInvalidValue, "pass_b_shape not compiled for this window size and epilogue"};
     variant = h->cfg.pass_b_shape;
   }
@@ -425,7 +483,19 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
   long long pairs = 0, launches = 0, dsum = 0;
   const int seq = (!h->capturing && h->n_seqs < gisspa_handle::kSeqs) ? h->n_seqs++ : -1;
   if (seq >= 0) GISSPA_CUDA(cudaEventRecord(h->qev[seq][0], c.s));
-  for (int n0 = 0; n0 < nt; n0 += D) {
+  const bool engine = !generic && variant == engine_variant(l);
+  if (engine) {
+    std::vector<Batch> batches;
+    for (int n0 = 0; n0 < nt; n0 += D)
+      for (int b0 = 0; b0 < W; b0 += E) {
+        batches.push_back(Batch{b0, n0, std::min(E, W - b0), std::min(D, nt - n0)});
+        pairs += (long long)batches.back().d * batches.back().e;
+        dsum += batches.back().d;
+      }
+    engine_sequence(c, epi, I, T, batches, D, E, args);
+    launches = (long long)batches.size();  // batches: the per-pass path's launch pairs
+  }
+  for (int n0 = 0; n0 < nt && !engine; n0 += D) {
     const int d = std::min(D, nt - n0);
     for (int b0 = 0; b0 < W; b0 += E) {
       const int e = std::min(E, W - b0);

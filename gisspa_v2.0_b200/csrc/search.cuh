@@ -79,6 +79,7 @@ struct gisspa_handle {
   gisspa::DevBuf S1, S2, peak, musig;
   // correlation intermediate and outputs
   gisspa::DevBuf Q, cand, cand_count, nn_key, nn_sum, zkey, zcand, zcount;
+  gisspa::DevBuf engine_ctr;  // work counters of the pair engine, one block per launch of a sequence
   gisspa::DevBuf gen_z, gen_x;  // workspace of the generic correlation (window sizes without tuned kernels)
   gisspa::DevBuf dev_err;  // set by kernels whose bounded waits gave up
   // adjoint: whitened template spectra before weighting, RMS factors, dW/dpsi tables,

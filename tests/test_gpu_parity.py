@@ -221,7 +221,7 @@ def test_chosen_form_picks_and_scores(name, tensor_cores):
     assert not rep["failures"], rep
 
 
-@pytest.mark.parametrize("name,shapes", [("norm_l256_w9", 2), ("norm_l512_w4", 4), ("norm_l1024_w4", 5)])
+@pytest.mark.parametrize("name,shapes", [("norm_l256_w9", 2), ("norm_l512_w4", 5), ("norm_l1024_w4", 5)])
 @pytest.mark.parametrize("mode", ["chunk", "topk"])
 def test_every_row_kernel_shape(name, shapes, mode):
     """Each compiled row-transform shape (forced with fixed launch batches) against the oracle."""
@@ -250,3 +250,34 @@ def test_tensor_core_column_pass_chunk_picks():
     assert len(o) > 0
     rep = check_chunk_picks(g, o, m, near, nm, cfg.threshold, rtol=1e-3, atol=0.0)
     assert not rep["failures"], rep
+
+
+@pytest.mark.parametrize("graphs", [1, 0])
+@pytest.mark.parametrize("mode", ["chunk", "topk", "fp16_topk"])
+def test_pair_engine_bit_identical_to_per_pass_kernels(mode, graphs):
+    """The pair engine (row shape 4 at window 512: pass A of one batch and pass B of the batch
+    before it in one launch, Q in two alternating slots) computes every value with the per-pass
+    kernels' device code and folds each batch into the per-pixel state in the same order: its
+    picks (and, for chunk picks, the mean / sigma maps) equal those of shape 0 bit for bit.  Uneven batches (4
+    templates in batches of 3, 4 windows in batches of 3), with and without CUDA graphs."""
+    img, tmpl, ctf, cfg = small_case("norm_l512_w4")
+    over = dict(template_batch=3, window_batch=3, cuda_graphs=graphs)
+    if mode != "chunk":
+        over.update(pick_mode=gisspa.PICK_TOPK, topk=20, exclusion_radius=30.0, threshold=2.0)
+    if mode == "fp16_topk":
+        over.update(spectrum_precision=gisspa.SPEC_FP16)
+    cfg = cfg.copy(**over)
+    res = []
+    for v in (0, 4):
+        s = gisspa.Searcher(cfg.copy(pass_b_shape=v))
+        s.set_templates(tmpl)
+        g = s.search(img, ctf)
+        W, L = 4, cfg.window_size
+        ms = stage(s, 5, None, ctf, 0.0, (W, L, L, 2), np.float32) if mode == "chunk" else None
+        res.append((g, ms, s.stats().pairs))
+        s.close()
+    (g0, ms0, p0), (g4, ms4, p4) = res
+    assert len(g0) > 0 and p0 == p4
+    assert np.array_equal(g0, g4)
+    if mode == "chunk":
+        assert np.array_equal(ms0, ms4)
