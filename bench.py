@@ -65,6 +65,8 @@ def args_parse():
                     help="launch every kernel from the host (cuda_graphs = 0), e.g. for per-launch profiling")
     ap.add_argument("--shape", type=int, default=-1,
                     help="with --batch: row-transform kernel shape (pass_b_shape) instead of the first")
+    ap.add_argument("--a-shape", type=int, default=-1,
+                    help="with --batch: column-transform kernel shape (pass_a_shape) instead of the first")
     ap.add_argument("--batch", default=None,
                     help="D,E: fix templates x windows per correlation launch instead of autotuning (profiling)")
     ap.add_argument("--chosen", default="fp16_topk", choices=list(FORMS) + ["none"],
@@ -447,6 +449,7 @@ def main():
     if a.batch:
         params["template_batch"], params["window_batch"] = (int(x) for x in a.batch.split(","))
         params["pass_b_shape"] = a.shape
+        params["pass_a_shape"] = a.a_shape
     if a.eager:
         params["cuda_graphs"] = 0
     params["tensor_cores"] = a.tensor_cores
@@ -586,7 +589,7 @@ def main():
                 "bytes_per_launch": alg, "bytes_per_pair": ba + bb, "launch_us": t_pair,
                 "pairs_per_launch": ppl, "templates_per_launch": dpl, "timed_launch_pairs": timed_pairs,
                 "launch_pairs_per_step": int(round(stats[-1].pairs / max(ppl, 1e-9))),
-                "pass_b_variant": int(stats[-1].pass_b_variant),
+                "pass_b_variant": int(stats[-1].pass_b_variant), "pass_a_variant": int(stats[-1].pass_a_variant),
                 "timing": "CUDA events around each host-launched angle's run of launch pairs (first angle of "
                           "each sweep), on the launching stream, inside the timed steps"}
 

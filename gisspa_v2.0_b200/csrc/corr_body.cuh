@@ -26,12 +26,17 @@ struct TeamSync {
   }
 };
 
-template <int L>
+// Pass A shapes: TT lanes per column, NC column slots per CTA, MINB CTAs per SM (the register
+// cap).  Window 512 has two: 16 lanes with 32 points each (a two-stage 32 x 16 plan, one
+// exchange, 128 registers) and 32 lanes with 16 points each (16 x 8 x 4, two exchanges, fewer
+// registers and twice the warps per SM).
+template <int L, int V = 0>
 struct PassA;
-template <> struct PassA<256> { static constexpr int TT = 16, NC = 16; };
-template <> struct PassA<320> { static constexpr int TT = 16, NC = 16; };
-template <> struct PassA<512> { static constexpr int TT = 16, NC = 16; };
-template <> struct PassA<1024> { static constexpr int TT = 32, NC = 8; };
+template <> struct PassA<256, 0> { static constexpr int TT = 16, NC = 16, MINB = 2; };
+template <> struct PassA<320, 0> { static constexpr int TT = 16, NC = 16, MINB = 2; };
+template <> struct PassA<512, 0> { static constexpr int TT = 16, NC = 16, MINB = 2; };
+template <> struct PassA<512, 1> { static constexpr int TT = 32, NC = 8, MINB = 4; };
+template <> struct PassA<1024, 0> { static constexpr int TT = 32, NC = 8, MINB = 2; };
 
 // The column transform of pass A: two Stockham stages (one exchange) for the powers of two,
 // three (20 x 4 x 4, two exchanges) for 320, whose 20 points per lane allow no two-stage plan
@@ -42,6 +47,14 @@ struct ColXform {
   __device__ __forceinline__ static int out_index(int tid, int e) { return fft2_out_index<L, TT>(tid, e); }
   __device__ __forceinline__ static void run(float2* v, float2* sm, const float2* tw, int tid) {
     fft2s<L, TT, +1>(v, sm, TwGlobal{tw}, tid, WarpSync{});
+  }
+};
+template <>
+struct ColXform<512, 32> {
+  __device__ __forceinline__ static int in_index(int tid, int e) { return fft3_in_index<512, 32>(tid, e); }
+  __device__ __forceinline__ static int out_index(int tid, int e) { return fft3_out_index<512, 32>(tid, e); }
+  __device__ __forceinline__ static void run(float2* v, float2* sm, const float2* tw, int tid) {
+    fft3<512, 32, +1>(v, sm, TwGlobal{tw}, tid, WarpSync{});
   }
 };
 template <>
@@ -62,12 +75,12 @@ struct ColXform<320, 16> {
 // of NC slots leaves as contiguous 16-byte stores.  The swizzle key is y >> SH with 16 / NC =
 // 2^SH rows per 128-byte line, so 16 consecutive rows of one column fall in 16 distinct bank
 // pairs.
-template <int L, typename SPEC>
+template <int L, typename SPEC, int V = 0>
 __device__ __forceinline__ void pass_a_body(float2* smem, const float2* __restrict__ I,
                                             const typename SPEC::T* __restrict__ T, float2* __restrict__ Q, int b0,
                                             int n0, int D, const float2* __restrict__ twL, int p, int cgroup,
                                             bool wait_before_store) {
-  constexpr int TT = PassA<L>::TT, NC = PassA<L>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
+  constexpr int TT = PassA<L, V>::TT, NC = PassA<L, V>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
   using CX = ColXform<L, TT>;
   constexpr int SH = NC >= 16 ? 0 : NC == 8 ? 1 : 2;
   static_assert(NC == 4 || NC == 8 || NC == 16, "swizzle assumes 4, 8 or 16 slots per CTA");
@@ -107,6 +120,8 @@ __device__ __forceinline__ void pass_a_body(float2* smem, const float2* __restri
   if (wait_before_store) griddep_wait();  // Q is still being read by the previous pass B
   float2* Qp = Q + (size_t)p * L * NZ + c0;
   constexpr int HALF = NC / 2;  // 16-byte pairs per row segment
+  // (a runtime loop: unrolled, with the swizzle at 16-byte granularity so that no pair needs
+  // its halves swapped, the launch pair measured 75.0 against 69.9 us at window 512)
   for (int u = threadIdx.x; u < L * HALF; u += TT * NC) {
     const int y = u / HALF, k = (u - y * HALF) * 2, sw = (y >> SH) & (NC - 1);
     const float4 q = *reinterpret_cast<const float4*>(smem + y * NC + ((k ^ sw) & ~1));
@@ -153,8 +168,10 @@ struct RowXform {
   template <typename Sync>
   __device__ __forceinline__ static void run(float2* v, float2* row, const float2* tw_nz, const float2* tw_l, int lt,
                                              Sync tsync) {
+    // only a lane's first input can be the row's slot 0 (lane 0)
+    v[0] = row_unpack<NZ>(row, tw_l, fft3_in_index<NZ, TEAM>(lt, 0));
 #pragma unroll
-    for (int i = 0; i < EIN; ++i) v[i] = row_unpack<NZ>(row, tw_l, fft3_in_index<NZ, TEAM>(lt, i));
+    for (int i = 1; i < EIN; ++i) v[i] = row_unpack<NZ, false>(row, tw_l, fft3_in_index<NZ, TEAM>(lt, i));
     tsync();  // every lane of the team has read the row before the transform overwrites it
     fft3<NZ, TEAM, +1>(v, row, TwShared{tw_nz}, lt, tsync);
   }
@@ -172,8 +189,9 @@ struct RowXform<320, 16> {
   __device__ __forceinline__ static void run(float2* v, float2* row, const float2* tw_nz, const float2* tw_l, int lt,
                                              Sync tsync) {
     if (lt < 10) {
+      v[0] = row_unpack<NZ>(row, tw_l, lt);
 #pragma unroll
-      for (int m = 0; m < EIN; ++m) v[m] = row_unpack<NZ>(row, tw_l, lt + 10 * m);
+      for (int m = 1; m < EIN; ++m) v[m] = row_unpack<NZ, false>(row, tw_l, lt + 10 * m);
     }
     tsync();
     if (lt < 10) {

@@ -9,14 +9,14 @@ namespace gisspa {
 namespace {
 
 // Pass A kernel: one pair per blockIdx.y, NC column slots per blockIdx.x (pass_a_body).
-template <int L, typename SPEC>
-__global__ void __launch_bounds__(PassA<L>::TT * PassA<L>::NC, 2)
+template <int L, typename SPEC, int V>
+__global__ void __launch_bounds__(PassA<L, V>::TT * PassA<L, V>::NC, PassA<L, V>::MINB)
     pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
                   int b0, int n0, int D, const float2* __restrict__ twL, int chained) {
   extern __shared__ __align__(16) float2 smem[];  // [NC * L]: FFT exchange buffers, then the output tile
   griddep_launch_dependents();
   if (!chained) griddep_wait();  // the spectra may come from the kernel just before
-  pass_a_body<L, SPEC>(smem, I, T, Q, b0, n0, D, twL, blockIdx.y, blockIdx.x, chained != 0);
+  pass_a_body<L, SPEC, V>(smem, I, T, Q, b0, n0, D, twL, blockIdx.y, blockIdx.x, chained != 0);
 }
 
 // Pass B: a team (TEAM lanes) per output row; RB rows per CTA, one window per blockIdx.y,
@@ -83,24 +83,27 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
   for (int i = 0; i < E; ++i) ox[i] = (2 * RX::out_index(lt, i) + L / 2) % L;
 
-  float acc1[RPT][E][2], acc2[RPT][E][2];
+  // per-pixel sums as pairs (pixels 2j, 2j + 1 of output element j): one paired FP32
+  // instruction adds a row's two values, with the rounding of two scalar additions
+  float2 acc1[RPT][E], acc2[RPT][E];
   float best[(EPI == EPI_TOPK) ? RPT : 1][E][2];
   int barg[(EPI == EPI_TOPK) ? RPT : 1][E][2];
-  float2 ms[(EPI == EPI_CHUNK) ? RPT : 1][E][2];
+  float2 mu[(EPI == EPI_CHUNK) ? RPT : 1][E], isg[(EPI == EPI_CHUNK) ? RPT : 1][E];
   if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll
     for (int s = 0; s < RPT; ++s)
 #pragma unroll
-      for (int i = 0; i < E; ++i)
+      for (int i = 0; i < E; ++i) {
+        acc1[s][i] = make_float2(0.f, 0.f);
+        acc2[s][i] = make_float2(0.f, 0.f);
+        if constexpr (EPI == EPI_TOPK) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          acc1[s][i][h] = 0.f;
-          acc2[s][i][h] = 0.f;
-          if constexpr (EPI == EPI_TOPK) {
+          for (int h = 0; h < 2; ++h) {
             best[s][i][h] = -INFINITY;
             barg[s][i][h] = -1;
           }
         }
+      }
   }
   if constexpr (EPI == EPI_CHUNK) {
 #pragma unroll
@@ -110,8 +113,8 @@ __global__ void __launch_bounds__(NW * 32, MINB)
       for (int i = 0; i < E; ++i) {
         const float4 m = *reinterpret_cast<const float4*>(a.musig + wbase + (size_t)oy * L + ox[i]);
         // (mu L^2, (1/sigma) / L^2): z = (raw - mu L^2) (1/sigma) / L^2 = (c - mu) / sigma exactly
-        ms[s][i][0] = make_float2(m.x * (float)(L * L), m.y * inv);
-        ms[s][i][1] = make_float2(m.z * (float)(L * L), m.w * inv);
+        mu[s][i] = make_float2(m.x * (float)(L * L), m.z * (float)(L * L));
+        isg[s][i] = make_float2(m.y * inv, m.w * inv);
       }
     }
   }
@@ -146,19 +149,21 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 
       if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll
-        for (int i = 0; i < E; ++i)
+        for (int i = 0; i < E; ++i) {
+          // raw values: the 1/L^2 is applied when folding
+          acc1[s][i] = cadd(acc1[s][i], v[i]);
+          acc2[s][i] = pfma(v[i], v[i], acc2[s][i]);
+          if constexpr (EPI == EPI_TOPK) {
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const float c = h ? v[i].y : v[i].x;  // raw: the 1/L^2 is applied when folding
-            acc1[s][i][h] += c;
-            acc2[s][i][h] = fmaf(c, c, acc2[s][i][h]);
-            if constexpr (EPI == EPI_TOPK) {
+            for (int h = 0; h < 2; ++h) {
+              const float c = h ? v[i].y : v[i].x;
               if (c > best[s][i][h]) {
                 best[s][i][h] = c;
                 barg[s][i][h] = angle * a.nt_total + a.n0 + d;
               }
             }
           }
+        }
       } else if constexpr (EPI == EPI_CHUNK) {
         // chunks (256 consecutive pixels of the window's linear index) touched by one row: whole
         // chunks for L a multiple of 256; at L = 320 a row starts 0, 64, 128 or 192 pixels into
@@ -175,13 +180,12 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         float z[E][2];
         float zmax = -INFINITY;
 #pragma unroll
-        for (int i = 0; i < E; ++i)
-#pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const float c = h ? v[i].y : v[i].x;
-            z[i][h] = (c - ms[s][i][h].x) * ms[s][i][h].y;
-            zmax = fmaxf(zmax, z[i][h]);
-          }
+        for (int i = 0; i < E; ++i) {
+          const float2 zz = pmul(csub(v[i], mu[s][i]), isg[s][i]);
+          z[i][0] = zz.x;
+          z[i][1] = zz.y;
+          zmax = fmaxf(zmax, fmaxf(zz.x, zz.y));
+        }
         // warp-uniform (and, for wide teams, team-uniform) branch: the shuffles below use the
         // full warp mask, so both half-warp teams (TEAM = 16) must enter together
         bool hit = __any_sync(0xffffffffu, zmax >= a.thresh);
@@ -314,8 +318,8 @@ __global__ void __launch_bounds__(NW * 32, MINB)
         const size_t pix = wbase + (size_t)oy * L + ox[i];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          atomicAdd(a.S1 + pix + h, (double)(acc1[s][i][h] * inv));
-          atomicAdd(a.S2 + pix + h, (double)(acc2[s][i][h] * (inv * inv)));
+          atomicAdd(a.S1 + pix + h, (double)((h ? acc1[s][i].y : acc1[s][i].x) * inv));
+          atomicAdd(a.S2 + pix + h, (double)((h ? acc2[s][i].y : acc2[s][i].x) * (inv * inv)));
           if constexpr (EPI == EPI_TOPK) {
             if (barg[s][i][h] >= 0)
               atomicMax(a.peak + pix + h, ((unsigned long long)float_key(best[s][i][h] * inv) << 32) |
@@ -345,18 +349,31 @@ void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaSt
   ++launch_counter();
 }
 
+template <int L, typename SPEC, int V>
+void launch_a_cfg(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
+                  const float2* twL, cudaStream_t s) {
+  constexpr int NZ = L / 2;
+  using P = PassA<L, V>;
+  constexpr size_t smem = (size_t)P::NC * L * sizeof(float2);
+  static PerDeviceOnce once;
+  once([] {
+    GISSPA_CUDA(
+        cudaFuncSetAttribute(pass_a_kernel<L, SPEC, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  });
+  dim3 grid(NZ / P::NC, cl.E * cl.D);
+  launch_pdl(pass_a_kernel<L, SPEC, V>, grid, dim3(P::TT * P::NC), smem, s, I,
+             static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0);
+}
 template <int L, typename SPEC>
 void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
               const float2* twL, cudaStream_t s) {
-  constexpr int NZ = L / 2;
-  constexpr size_t smem = (size_t)PassA<L>::NC * L * sizeof(float2);
-  static PerDeviceOnce once;
-  once([] {
-    GISSPA_CUDA(cudaFuncSetAttribute(pass_a_kernel<L, SPEC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  });
-  dim3 grid(NZ / PassA<L>::NC, cl.E * cl.D);
-  launch_pdl(pass_a_kernel<L, SPEC>, grid, dim3(PassA<L>::TT * PassA<L>::NC), smem, s, I,
-             static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0);
+  if constexpr (L == 512) {
+    if (cl.a_variant == 1) {
+      launch_a_cfg<L, SPEC, 1>(cl, I, T, Q, args, twL, s);
+      return;
+    }
+  }
+  launch_a_cfg<L, SPEC, 0>(cl, I, T, Q, args, twL, s);
 }
 
 template <int L, int TEAM, int RB, int NW, int EPI, int MINB>
@@ -476,6 +493,8 @@ int launch_pair(const CorrLaunch& cl, const float2* I, const void* T, float2* Q,
 }
 
 }  // namespace
+
+int pass_a_variants(int L) { return L == 512 ? 2 : 1; }
 
 bool correlate_supported(int L) { return L == 256 || L == 512 || L == 1024; }
 

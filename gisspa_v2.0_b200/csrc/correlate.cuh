@@ -75,6 +75,7 @@ struct CorrLaunch {
   int spec;           // GISSPA_SPEC_*
   int epi;            // Epilogue
   int variant = 0;    // pass B shape (see correlate_variants)
+  int a_variant = 0;  // pass A shape (see pass_a_variants)
   // Pass A directly follows the previous launch's pass B on the stream and reads nothing that
   // pass B writes: it then waits for it only before storing Q (programmatic dependent launch
   // overlaps the rest with pass B's last CTAs).  Otherwise pass A waits at its start.
@@ -108,6 +109,8 @@ void engine_launch(int spec, int epi, const float2* I, const void* T, const Engi
                    const CorrArgs& b_args, int* ctr, bool chained, const float2* twL, const float2* twNZ,
                    cudaStream_t s);
 
+// Number of pass A shapes compiled for a window size.
+int pass_a_variants(int L);
 // The pass B shape index that selects the pair engine at window size L (-1: none).
 int engine_variant(int L);
 
@@ -115,10 +118,11 @@ int engine_variant(int L);
 // One input of a row's half-length inverse transform: from the row's Hermitian half (slot 0
 // packing the kx = 0 and kx = L/2 terms as its real and imaginary parts), Z[k] = E[k] +
 // i W_L^-k O[k] with E, O the even and odd parts (tw_l: e^(-2 pi i k / L), k < NZ).
-template <int NZ>
+// MAYBE_ZERO = false: the caller knows k > 0 (every input of a lane but its first).
+template <int NZ, bool MAYBE_ZERO = true>
 __device__ __forceinline__ float2 row_unpack(const float2* row, const float2* tw_l, int k) {
   float2 xk, xm;
-  if (k == 0) {
+  if (MAYBE_ZERO && k == 0) {
     const float2 q = row[0];
     xk = make_float2(q.x, 0.f);
     xm = make_float2(q.y, 0.f);

@@ -59,29 +59,30 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
 #pragma unroll
   for (int i = 0; i < E; ++i) ox[i] = (2 * RX::out_index(lane, i) + kL / 2) % kL;
 
-  float acc1[E][2], acc2[E][2];
+  float2 acc1[E], acc2[E];  // pixels 2j, 2j + 1 of output element j as pairs
   float best[(EPI == EPI_TOPK) ? E : 1][2];
   int barg[(EPI == EPI_TOPK) ? E : 1][2];
-  float2 ms[(EPI == EPI_CHUNK) ? E : 1][2];
+  float2 mu[(EPI == EPI_CHUNK) ? E : 1], isg[(EPI == EPI_CHUNK) ? E : 1];
   if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll
-    for (int i = 0; i < E; ++i)
+    for (int i = 0; i < E; ++i) {
+      acc1[i] = make_float2(0.f, 0.f);
+      acc2[i] = make_float2(0.f, 0.f);
+      if constexpr (EPI == EPI_TOPK) {
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        acc1[i][h] = 0.f;
-        acc2[i][h] = 0.f;
-        if constexpr (EPI == EPI_TOPK) {
+        for (int h = 0; h < 2; ++h) {
           best[i][h] = -INFINITY;
           barg[i][h] = -1;
         }
       }
+    }
   }
   if constexpr (EPI == EPI_CHUNK) {
 #pragma unroll
     for (int i = 0; i < E; ++i) {
       const float4 m = *reinterpret_cast<const float4*>(a.musig + wbase + (size_t)oy * kL + ox[i]);
-      ms[i][0] = make_float2(m.x * (float)(kL * kL), m.y * inv);
-      ms[i][1] = make_float2(m.z * (float)(kL * kL), m.w * inv);
+      mu[i] = make_float2(m.x * (float)(kL * kL), m.z * (float)(kL * kL));
+      isg[i] = make_float2(m.y * inv, m.w * inv);
     }
   }
 
@@ -120,32 +121,32 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
 
     if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
 #pragma unroll
-      for (int i = 0; i < E; ++i)
+      for (int i = 0; i < E; ++i) {
+        acc1[i] = cadd(acc1[i], v[i]);  // raw: the 1/L^2 is applied when folding
+        acc2[i] = pfma(v[i], v[i], acc2[i]);
+        if constexpr (EPI == EPI_TOPK) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const float c = h ? v[i].y : v[i].x;  // raw: the 1/L^2 is applied when folding
-          acc1[i][h] += c;
-          acc2[i][h] = fmaf(c, c, acc2[i][h]);
-          if constexpr (EPI == EPI_TOPK) {
+          for (int h = 0; h < 2; ++h) {
+            const float c = h ? v[i].y : v[i].x;
             if (c > best[i][h]) {
               best[i][h] = c;
               barg[i][h] = angle * a.nt_total + a.n0 + d;
             }
           }
         }
+      }
     } else if constexpr (EPI == EPI_CHUNK) {
       constexpr int CPR = kL / 256;
       const int c0 = (oy * kL) >> 8;
       float z[E][2];
       float zmax = -INFINITY;
 #pragma unroll
-      for (int i = 0; i < E; ++i)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const float c = h ? v[i].y : v[i].x;
-          z[i][h] = (c - ms[i][h].x) * ms[i][h].y;
-          zmax = fmaxf(zmax, z[i][h]);
-        }
+      for (int i = 0; i < E; ++i) {
+        const float2 zz = pmul(csub(v[i], mu[i]), isg[i]);
+        z[i][0] = zz.x;
+        z[i][1] = zz.y;
+        zmax = fmaxf(zmax, fmaxf(zz.x, zz.y));
+      }
       if (__any_sync(0xffffffffu, zmax >= a.thresh)) {
 #pragma unroll
         for (int ch = 0; ch < CPR; ++ch) {
@@ -174,8 +175,8 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
       const size_t pix = wbase + (size_t)oy * kL + ox[i];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        atomicAdd(a.S1 + pix + h, (double)(acc1[i][h] * inv));
-        atomicAdd(a.S2 + pix + h, (double)(acc2[i][h] * (inv * inv)));
+        atomicAdd(a.S1 + pix + h, (double)((h ? acc1[i].y : acc1[i].x) * inv));
+        atomicAdd(a.S2 + pix + h, (double)((h ? acc2[i].y : acc2[i].x) * (inv * inv)));
         if constexpr (EPI == EPI_TOPK) {
           if (barg[i][h] >= 0)
             atomicMax(a.peak + pix + h, ((unsigned long long)float_key(best[i][h] * inv) << 32) |

@@ -94,6 +94,10 @@ int validate_config(const gisspa_config& c, std::string& err) {
           " shapes compiled for window_size " + std::to_string(l);
     return GISSPA_ERR_ARG;
   }
+  if (c.pass_a_shape < -1 || c.pass_a_shape >= (correlate_fast(l) ? pass_a_variants(l) : 1)) {
+    err = "pass_a_shape must be -1 or one of the shapes compiled for window_size " + std::to_string(l);
+    return GISSPA_ERR_ARG;
+  }
   if (c.pass_b_shape >= 0) {
     const int epis[3] = {c.norm_type == 0 ? EPI_NONORM : (c.pick_mode == GISSPA_PICK_TOPK ? EPI_TOPK : EPI_SUM),
                          c.norm_type == 0 ? EPI_NONORM : EPI_CHUNK, EPI_MAP};
@@ -359,6 +363,8 @@ bool engine_ok(const gisspa_config& cfg, int l, int epi) {
   return engine_supported(l, epi) && !(cfg.tensor_cores && cfg.spectrum_precision == GISSPA_SPEC_FP16);
 }
 
+constexpr bool kTuneEngine = false;
+
 // Autotuner: times every candidate launch shape (pass B variant, template batch D, window
 // batch E) on the sweep's own spectra, with the epilogue's outputs redirected to scratch,
 // and keeps the fastest per (window size, epilogue, precision).
@@ -405,10 +411,13 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   const float2* twNZ = h->fft.twiddles(l / 2);
   TuneChoice best;
   best.us_per_pair = 1e30;
+  const size_t tbytes = spec_bytes(h->cfg.spectrum_precision) * (size_t)(l / 2 + 1) * l;  // one template
   for (int v = 0; v < correlate_variants(l); ++v)
     for (const auto& cd : cands) {
       if (v == engine_variant(l)) {
-        if (!engine_ok(h->cfg, l, epi)) continue;
+        // measured slower than the per-pass kernels on B200 (83.6 against 70.0 us per batch of
+        // 96 pairs at window 512): selectable with pass_b_shape, not tuned
+        if (!kTuneEngine || !engine_ok(h->cfg, l, epi)) continue;
         // the engine runs whole sequences: kReps batches (kReps + 1 launches) of the same pairs
         constexpr int kReps = 4;
         const std::vector<Batch> seq(kReps, Batch{0, 0, cd.E, cd.D});
@@ -425,21 +434,34 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
         continue;
       }
       if (!correlate_variant_ok(l, v, epi)) continue;
-      CorrLaunch cl{l, cd.E, cd.D, h->cfg.spectrum_precision, epi, v};
-      cl.tc = h->cfg.tensor_cores != 0;
-      args.b0 = 0;
-      args.n0 = 0;
-      args.D = cd.D;
-      correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s);
-      GISSPA_CUDA(cudaEventRecord(h->ev[5], c.s));
-      constexpr int kReps = 3;
-      for (int r = 0; r < kReps; ++r) correlate_launch(cl, I, T, Q, args, twL, twNZ, c.s);
-      GISSPA_CUDA(cudaEventRecord(h->ev[6], c.s));
-      GISSPA_CUDA(cudaEventSynchronize(h->ev[6]));
-      float ms = 0;
-      GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
-      const double us = 1000.0 * ms / (kReps * cd.D * cd.E);
-      if (us < best.us_per_pair) best = TuneChoice{v, cd.D, cd.E, us};
+      for (int av = 0; av < pass_a_variants(l); ++av) {
+        CorrLaunch cl{l, cd.E, cd.D, h->cfg.spectrum_precision, epi, v};
+        cl.tc = h->cfg.tensor_cores != 0;
+        cl.a_variant = av;
+        args.D = cd.D;
+        // each timed launch on other windows and templates than the one before (where the
+        // search has them), so that its spectra come from HBM as in a sweep, not from L2: the
+        // spectra pointers move, the outputs stay on the scratch state of windows 0 .. E - 1
+        args.b0 = 0;
+        args.n0 = 0;
+        auto at = [&](int r) {
+          const int b0 = W > cd.E ? (r * cd.E) % (W - cd.E + 1) : 0;
+          const int n0 = nt > cd.D ? (r * cd.D) % (nt - cd.D + 1) : 0;
+          cl.chained = r > 0;
+          correlate_launch(cl, I + (size_t)b0 * (l / 2 + 1) * l,
+                           static_cast<const char*>(T) + (size_t)n0 * tbytes, Q, args, twL, twNZ, c.s);
+        };
+        at(0);
+        GISSPA_CUDA(cudaEventRecord(h->ev[5], c.s));
+        constexpr int kReps = 3;
+        for (int r = 1; r <= kReps; ++r) at(r);
+        GISSPA_CUDA(cudaEventRecord(h->ev[6], c.s));
+        GISSPA_CUDA(cudaEventSynchronize(h->ev[6]));
+        float ms = 0;
+        GISSPA_CUDA(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
+        const double us = 1000.0 * ms / (kReps * cd.D * cd.E);
+        if (us < best.us_per_pair) best = TuneChoice{v, cd.D, cd.E, us, av};
+      }
     }
   return best;
 }
@@ -448,7 +470,7 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
 long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, int nt, CorrArgs args, int D, int E) {
   gisspa_handle* h = c.h;
   const int l = c.l;
-  int variant = 0;
+  int variant = 0, a_variant = 0;
   const bool generic = !correlate_fast(l);  // no hand-tuned kernels for this window size
   if (!generic && h->cfg.template_batch > 0 && h->cfg.window_batch > 0 && h->cfg.pass_b_shape >= 0) {
     if (!correlate_variant_ok(l, h->cfg.pass_b_shape, epi) ||
@@ -456,6 +478,8 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
       throw CudaError{cudaErrorInvalidValue, "pass_b_shape not compiled for this window size and epilogue"};
     variant = h->cfg.pass_b_shape;
   }
+  if (!generic && h->cfg.template_batch > 0 && h->cfg.window_batch > 0 && h->cfg.pass_a_shape >= 0)
+    a_variant = h->cfg.pass_a_shape;
   if (!generic && h->cfg.template_batch == 0 && h->cfg.window_batch == 0) {
     const long long key = (long long)l | ((long long)epi << 16) | ((long long)h->cfg.spectrum_precision << 24) |
                           ((long long)std::min(nt, 64) << 32) | ((long long)std::min(W, 64) << 40);
@@ -464,7 +488,9 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
     D = it->second.D;
     E = it->second.E;
     variant = it->second.variant;
+    a_variant = it->second.a_variant;
     h->st.pass_b_variant = variant;
+    h->st.pass_a_variant = a_variant;
     h->st.tuned_us_per_pair = it->second.us_per_pair;
   }
   float2* Q = nullptr;
@@ -501,6 +527,7 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
       const int e = std::min(E, W - b0);
       CorrLaunch cl{l, e, d, h->cfg.spectrum_precision, epi, variant};
       cl.tc = h->cfg.tensor_cores != 0;
+      cl.a_variant = a_variant;
       cl.chained = pairs > 0;  // after this sequence's first pair of passes
       args.Q = Q;
       args.b0 = b0;

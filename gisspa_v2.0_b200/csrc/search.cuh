@@ -17,6 +17,7 @@ namespace gisspa {
 struct TuneChoice {
   int variant = 0, D = 1, E = 1;
   double us_per_pair = 0;
+  int a_variant = 0;  // pass A shape
 };
 
 // One norm_type=1 search between its phases: preparation, sweeps over angle ranges, the

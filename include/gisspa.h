@@ -86,6 +86,9 @@ typedef struct gisspa_config {
                              run on the tensor cores (tcgen05, FP16 operands, FP32 accumulation;
                              same picks, scores within 1.1e-4 of the FP32 form) -- measured 1.7x
                              slower per launch pair than 0 on B200; 0 (default): CUDA cores */
+  int pass_a_shape;       /* with template_batch and window_batch set: column-transform kernel shape
+                             (0 .. compiled shapes - 1: two at window 512, one elsewhere; -1 = the
+                             first); ignored when autotuning */
 } gisspa_config;
 
 /* Per-micrograph CTF, as in an LST line "defocus= dfdiff= dfang=" (DataReader2.h:93-103).
@@ -134,13 +137,15 @@ typedef struct gisspa_stats {
   double templates_per_launch; /* mean template batch depth D per launch of the search */
   int pass_samples;
   int window_size;
-  int pass_b_variant;          /* pass B shape picked by the autotuner (last sweep) */
+  int pass_b_variant;          /* pass B shape picked by the autotuner (last sweep); at window 512
+                                  shape 4 is the pair engine (both passes in one launch) */
   double tuned_us_per_pair;    /* autotuner's measured time per pair of that shape */
   long long graph_replays;     /* angles run as replays of a captured CUDA graph */
   /* CUDA events around whole runs of correlation launches (every host-launched angle: the
    * first of each sweep when graphs are on), nothing recorded between them */
   double corr_pair_us;         /* mean duration of one pass A + pass B launch pair */
   long long corr_timed_launches; /* launch pairs inside those runs */
+  int pass_a_variant;          /* pass A shape picked by the autotuner (last sweep) */
 } gisspa_stats;
 
 typedef struct gisspa_handle gisspa_handle;

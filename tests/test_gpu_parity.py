@@ -221,10 +221,12 @@ def test_chosen_form_picks_and_scores(name, tensor_cores):
     assert not rep["failures"], rep
 
 
-@pytest.mark.parametrize("name,shapes", [("norm_l256_w9", 2), ("norm_l512_w4", 5), ("norm_l1024_w4", 5)])
+@pytest.mark.parametrize("name,shapes,a_shapes", [("norm_l256_w9", 2, 1), ("norm_l512_w4", 5, 2),
+                                                  ("norm_l1024_w4", 5, 1)])
 @pytest.mark.parametrize("mode", ["chunk", "topk"])
-def test_every_row_kernel_shape(name, shapes, mode):
-    """Each compiled row-transform shape (forced with fixed launch batches) against the oracle."""
+def test_every_row_kernel_shape(name, shapes, a_shapes, mode):
+    """Each compiled row-transform shape, and at window 512 each column-transform shape (forced
+    with fixed launch batches), against the oracle."""
     img, tmpl, ctf, cfg = small_case(name)
     over = dict(template_batch=2, window_batch=2)
     if mode == "topk":
@@ -232,15 +234,15 @@ def test_every_row_kernel_shape(name, shapes, mode):
     cfg = cfg.copy(**over)
     o, m, near, nm = oracle.search(cfg, ctf, img, tmpl, want_margins=True)
     assert len(o) > 0
-    for v in range(shapes):
-        s = gisspa.Searcher(cfg.copy(pass_b_shape=v))
+    for v, av in [(v, 0) for v in range(shapes)] + [(0, av) for av in range(1, a_shapes)]:
+        s = gisspa.Searcher(cfg.copy(pass_b_shape=v, pass_a_shape=av))
         s.set_templates(tmpl)
         g = s.search(img, ctf)
         if mode == "chunk":
             rep = check_chunk_picks(g, o, m, near, nm, cfg.threshold)
         else:
             rep = check_topk_picks(g, o, m)
-        assert not rep["failures"], (v, rep)
+        assert not rep["failures"], (v, av, rep)
 
 
 def test_tensor_core_column_pass_chunk_picks():
