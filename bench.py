@@ -55,6 +55,8 @@ def args_parse():
     ap.add_argument("--form", default="plain", choices=list(FORMS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-full-sweeps", action="store_true",
+                    help="skip timing the plain form with every row of sweep 2 transformed (prune_sweep2=0)")
     ap.add_argument("--no-precision-check", action="store_true",
                     help="skip the untimed FP32 / BF16 top-K searches that measure the chosen form's score error")
     ap.add_argument("--no-reference-cuda", action="store_true",
@@ -427,6 +429,18 @@ def bench_project(a, rank: int, local: int):
 
 
 # ------------------------------------------------------------------ main
+def same_picks(a: np.ndarray, b: np.ndarray) -> dict:
+    """Two pick lists of one micrograph: whether they hold the same (x, y, template, angle) picks,
+    and the largest relative score difference between matching picks (two searches may tune
+    different launch shapes, whose rounding differs in the last bits)."""
+    key = lambda p: (float(p["x"]), float(p["y"]), int(p["template_id"]), int(p["angle_index"]))
+    da = {key(p): float(p["score"]) for p in a}
+    db = {key(p): float(p["score"]) for p in b}
+    common = set(da) & set(db)
+    rel = max((abs(da[k] - db[k]) / max(abs(db[k]), 1e-30) for k in common), default=0.0)
+    return {"n": [len(a), len(b)], "same": len(a) == len(b) and set(da) == set(db), "max_rel_score_diff": rel}
+
+
 def main():
     a = args_parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -591,7 +605,34 @@ def main():
                 "launch_pairs_per_step": int(round(stats[-1].pairs / max(ppl, 1e-9))),
                 "pass_b_variant": int(stats[-1].pass_b_variant), "pass_a_variant": int(stats[-1].pass_a_variant),
                 "timing": "CUDA events around each host-launched angle's run of launch pairs (first angle of "
-                          "each sweep), on the launching stream, inside the timed steps"}
+                          "each sweep; a pruned second sweep, which skips rows, is left out), on the "
+                          "launching stream, inside the timed steps"}
+
+    # the plain form again with every row of sweep 2 transformed (prune_sweep2 = 0): the same
+    # picks, the work of two full sweeps
+    full = None
+    if a.form == "plain" and cfg.norm_type == 1 and cfg.pick_mode == gisspa.PICK_CHUNK and not a.no_full_sweeps:
+        pruned_picks = out[:npicks].copy()
+        s3 = gisspa.Searcher(cfg.copy(prune_sweep2=0), local)
+        s3.set_templates(case.templates)
+        for _ in range(a.warmup):
+            s3.search_device(d_img.data_ptr(), nx, ny, ctf, out)
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(a.steps):
+            n3 = s3.search_device(d_img.data_ptr(), nx, ny, ctf, out)
+        ev1.record()
+        torch.cuda.synchronize()
+        barrier()
+        t3 = torch.tensor([ev0.elapsed_time(ev1)], device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t3, op=torch.distributed.ReduceOp.MAX)
+        full = {"value": world * a.steps / (float(t3.item()) / 1000.0), "unit": "micrographs/s",
+                "ms_per_step": float(t3.item()) / a.steps, "picks_per_step": int(n3),
+                "same_picks_as_pruned": same_picks(out[:n3], pruned_picks),
+                "stage_ms": {"sweep1": s3.stats().ms_sweep1, "sweep2": s3.stats().ms_sweep2}}
+        s3.close()
 
     # the chosen form on the same micrograph: FP16 spectra, one top-K sweep (the numerator of
     # the target ratio against the plain FP32 two-sweep form timed above)
@@ -619,7 +660,8 @@ def main():
         st2 = s2.stats()
         chosen_picks = out[:n2].copy()
         chosen = {"form": a.chosen, "value": v2, "unit": "micrographs/s", "ms_per_step": float(t2.item()) / a.steps,
-                  "vs_plain": v2 / value, "picks_per_step": int(n2), "launch_pair_us": st2.corr_pair_us,
+                  "vs_plain": v2 / value, "vs_plain_full_sweeps": v2 / full["value"] if full else None,
+                  "picks_per_step": int(n2), "launch_pair_us": st2.corr_pair_us,
                   "pairs_per_launch": st2.pairs_per_launch}
         s2.close()
         if not a.no_precision_check:
@@ -638,7 +680,8 @@ def main():
                "stage_ms": {"prep": stats[-1].ms_prep, "sweep1": stats[-1].ms_sweep1,
                             "sweep2": stats[-1].ms_sweep2, "pick": stats[-1].ms_pick},
                "gpu_launches": int(launches), "graph_replays": int(stats[-1].graph_replays), "clocks": clk,
-               "roofline": roofline, "e2e": e2e}
+               "roofline": roofline, "e2e": e2e, "rows_alive": float(stats[-1].rows_alive),
+               "plain_full_sweeps": full}
         if chosen is not None:
             res["chosen_form"] = chosen
         if world == 1 and not a.no_cpu_baseline:

@@ -54,6 +54,7 @@ void gisspa_config_default(gisspa_config* c) {
   c->pass_b_shape = -1;
   c->tensor_cores = 0;
   c->pass_a_shape = -1;
+  c->prune_sweep2 = 1;
 }
 
 int gisspa_create(const gisspa_config* cfg, int device, gisspa_handle** out) {

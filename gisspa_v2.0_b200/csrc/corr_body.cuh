@@ -79,7 +79,8 @@ template <int L, typename SPEC, int V = 0>
 __device__ __forceinline__ void pass_a_body(float2* smem, const float2* __restrict__ I,
                                             const typename SPEC::T* __restrict__ T, float2* __restrict__ Q, int b0,
                                             int n0, int D, const float2* __restrict__ twL, int p, int cgroup,
-                                            bool wait_before_store) {
+                                            bool wait_before_store, const unsigned char* __restrict__ alive,
+                                            const unsigned char* __restrict__ alive_win) {
   constexpr int TT = PassA<L, V>::TT, NC = PassA<L, V>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
   using CX = ColXform<L, TT>;
   constexpr int SH = NC >= 16 ? 0 : NC == 8 ? 1 : 2;
@@ -88,6 +89,10 @@ __device__ __forceinline__ void pass_a_body(float2* smem, const float2* __restri
   const int team = threadIdx.x / TT, tid = threadIdx.x - team * TT;
   const int c0 = cgroup * NC, c = c0 + team;
   const int e = p / D, d = p - e * D;
+  if (alive_win && !alive_win[b0 + e]) {  // no row of this window is needed (CTA-uniform)
+    if (wait_before_store) griddep_wait();  // complete only after the kernel before, as when storing
+    return;
+  }
   const float2* Ib = I + (size_t)(b0 + e) * HS * L;
   const typename SPEC::T* Tn = T + (size_t)(n0 + d) * HS * L;
   float2 v[E];
@@ -122,8 +127,10 @@ __device__ __forceinline__ void pass_a_body(float2* smem, const float2* __restri
   constexpr int HALF = NC / 2;  // 16-byte pairs per row segment
   // (a runtime loop: unrolled, with the swizzle at 16-byte granularity so that no pair needs
   // its halves swapped, the launch pair measured 75.0 against 69.9 us at window 512)
+  const unsigned char* live = alive ? alive + (size_t)(b0 + e) * L : nullptr;
   for (int u = threadIdx.x; u < L * HALF; u += TT * NC) {
     const int y = u / HALF, k = (u - y * HALF) * 2, sw = (y >> SH) & (NC - 1);
+    if (live && !live[y]) continue;  // a row the next pass skips
     const float4 q = *reinterpret_cast<const float4*>(smem + y * NC + ((k ^ sw) & ~1));
     *reinterpret_cast<float4*>(Qp + (size_t)y * NZ + k) =
         (sw & 1) ? make_float4(q.z, q.w, q.x, q.y) : q;

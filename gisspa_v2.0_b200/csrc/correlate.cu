@@ -12,11 +12,12 @@ namespace {
 template <int L, typename SPEC, int V>
 __global__ void __launch_bounds__(PassA<L, V>::TT * PassA<L, V>::NC, PassA<L, V>::MINB)
     pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
-                  int b0, int n0, int D, const float2* __restrict__ twL, int chained) {
+                  int b0, int n0, int D, const float2* __restrict__ twL, int chained,
+                  const unsigned char* __restrict__ alive, const unsigned char* __restrict__ alive_win) {
   extern __shared__ __align__(16) float2 smem[];  // [NC * L]: FFT exchange buffers, then the output tile
   griddep_launch_dependents();
   if (!chained) griddep_wait();  // the spectra may come from the kernel just before
-  pass_a_body<L, SPEC, V>(smem, I, T, Q, b0, n0, D, twL, blockIdx.y, blockIdx.x, chained != 0);
+  pass_a_body<L, SPEC, V>(smem, I, T, Q, b0, n0, D, twL, blockIdx.y, blockIdx.x, chained != 0, alive, alive_win);
 }
 
 // Pass B: a team (TEAM lanes) per output row; RB rows per CTA, one window per blockIdx.y,
@@ -44,6 +45,18 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   }
   const int team = threadIdx.x / TEAM, lt = threadIdx.x - team * TEAM;
   const int e = blockIdx.y, y0 = blockIdx.x * RB, win = a.b0 + e;
+  if constexpr (EPI == EPI_CHUNK) {
+    // rows that cannot hold a pick are skipped; a CTA with none left leaves at once, after the
+    // pass A before it has completed (so that this kernel completes after it, as when it reads Q)
+    if (a.alive) {
+      bool any = false;
+      for (int r = 0; r < RB; ++r) any = any || a.alive[(size_t)win * L + y0 + r] != 0;
+      if (!any) {
+        griddep_wait();
+        return;
+      }
+    }
+  }
   const int angle = a.angle_state ? a.angle_state->index : a.angle;
   // L = 320: the CTA's output rows (L/2 + y0 ...) hold whole chunks (RB a multiple of 4 that
   // divides L/2: 4 rows = 5 chunks, and the rows never wrap inside one CTA); their maxima are
@@ -142,6 +155,11 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     for (int s = 0; s < RPT; ++s) {
       const int r = team + NTEAM * s;
       const int oy = (y0 + r + L / 2) % L;
+      // a dead row (pass A did not store it) is skipped by its team; half-warp teams stay in
+      // step (the chunk vote uses the whole warp): they transform it and discard its values
+      const bool row_live = EPI != EPI_CHUNK || !a.alive || a.alive[(size_t)win * L + y0 + r];
+      if constexpr (EPI == EPI_CHUNK && TEAM >= 32)
+        if (!row_live) continue;
       float2* row = stg + r * NZ;
       float2 v[RX::EBUF];
       const TeamSync<TEAM> tsync{1 + team};
@@ -182,9 +200,9 @@ __global__ void __launch_bounds__(NW * 32, MINB)
 #pragma unroll
         for (int i = 0; i < E; ++i) {
           const float2 zz = pmul(csub(v[i], mu[s][i]), isg[s][i]);
-          z[i][0] = zz.x;
-          z[i][1] = zz.y;
-          zmax = fmaxf(zmax, fmaxf(zz.x, zz.y));
+          z[i][0] = row_live ? zz.x : -INFINITY;
+          z[i][1] = row_live ? zz.y : -INFINITY;
+          zmax = fmaxf(zmax, fmaxf(z[i][0], z[i][1]));
         }
         // warp-uniform (and, for wide teams, team-uniform) branch: the shuffles below use the
         // full warp mask, so both half-warp teams (TEAM = 16) must enter together
@@ -362,7 +380,8 @@ void launch_a_cfg(const CorrLaunch& cl, const float2* I, const void* T, float2* 
   });
   dim3 grid(NZ / P::NC, cl.E * cl.D);
   launch_pdl(pass_a_kernel<L, SPEC, V>, grid, dim3(P::TT * P::NC), smem, s, I,
-             static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0);
+             static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0,
+             cl.epi == EPI_CHUNK ? args.alive : nullptr, cl.epi == EPI_CHUNK ? args.alive_win : nullptr);
 }
 template <int L, typename SPEC>
 void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,

@@ -60,6 +60,10 @@ struct CorrArgs {
   Cand* cand;
   unsigned* cand_count;
   unsigned cand_cap;
+  // EPI_CHUNK (optional): the window rows that can still hold a pick, alive[window][y] by row of
+  // Q (output row (y + L/2) mod L), and alive_win[window]; rows and windows marked 0 are skipped
+  const unsigned char* alive;
+  const unsigned char* alive_win;
   // EPI_NONORM, indexed [window][template] with nt_total templates per window
   unsigned long long* nn_key;
   double* nn_sum;           // [W][nt_total][2]

@@ -51,6 +51,8 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
   using RX = RowXform<kL, 32>;
   constexpr int E = RX::EOUT;
   const int win = a.b0 + e;
+  if constexpr (EPI == EPI_CHUNK)
+    if (a.alive && !a.alive[(size_t)win * kL + y]) return true;  // a row that cannot hold a pick
   const int angle = a.angle_state ? a.angle_state->index : a.angle;
   const int oy = (y + kL / 2) % kL;
   const float inv = 1.0f / (float)(kL * kL);
@@ -227,7 +229,8 @@ __global__ void __launch_bounds__(kThreads, 2) pair_engine_kernel(EngineArgs g) 
         const int it = s_item[k & 1];
         if (it >= nitems) break;
         pass_a_body<kL, SPEC>(tile, g.I, static_cast<const typename SPEC::T*>(g.T), g.A.Q, g.A.b0, g.A.n0, g.A.d,
-                              g.twL, it / kGroups, it % kGroups, g.chained != 0);
+                              g.twL, it / kGroups, it % kGroups, g.chained != 0,
+                              EPI == EPI_CHUNK ? g.b.alive : nullptr, EPI == EPI_CHUNK ? g.b.alive_win : nullptr);
       }
     } else if ((phase == 0) != (role == 0) && g.B.valid) {
       // pass B rows: (window, row) of batch B, one warp per row

@@ -155,6 +155,41 @@ __global__ void peak_flip_kernel(const unsigned long long* __restrict__ in, long
   out[i] = in[i] ^ 0x8000000000000000ull;
 }
 
+// Rows that sweep 2 must transform.  Every pair's z at a pixel is at most the z of the pixel's
+// best correlation over all pairs (fl((c - mu) s) does not decrease with c for s >= 0), so a row
+// whose pixels all have a best z below the threshold holds no chunk pick for any template or
+// angle: the chunk maximum that reaches the threshold lies on a pixel whose best z does.  The
+// margin covers the rounding difference between this z (from the normalised best correlation)
+// and pass B's (from the raw transform).  One warp per row; alive[w][y] by row y of Q (output
+// row (y + l/2) mod l), alive_win[w] set when any row of window w is alive, *count += rows.
+constexpr float kAliveMargin = 1e-3f;
+__global__ void row_alive_kernel(const unsigned long long* __restrict__ peak, const float2* __restrict__ ms, int l,
+                                 long long rows, float thresh, unsigned char* __restrict__ alive,
+                                 unsigned char* __restrict__ alive_win, unsigned* __restrict__ count) {
+  const long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= rows) return;  // whole warps
+  const long long w = row / l;
+  const int y = (int)(row % l), oy = (y + l / 2) % l;
+  const size_t base = ((size_t)w * l + oy) * l;
+  bool hit = false;
+  for (int x = lane; x < l; x += 32) {
+    const unsigned long long pk = peak[base + x];
+    if (!pk) continue;
+    const float2 m = ms[base + x];
+    const float z = (key_float((uint32_t)(pk >> 32)) - m.x) * m.y;
+    hit = hit || z >= thresh - kAliveMargin;
+  }
+  hit = __any_sync(0xffffffffu, hit);
+  if (lane == 0) {
+    alive[row] = hit ? 1 : 0;
+    if (hit) {
+      alive_win[w] = 1;
+      atomicAdd(count, 1u);
+    }
+  }
+}
+
 // Top-K: image map of the max z over windows covering each pixel (ties: lowest window).
 __global__ void zmap_kernel(const unsigned long long* __restrict__ peak, const float2* __restrict__ ms, int l,
                             const int* __restrict__ offx, const int* __restrict__ offy, int bx, int nx, int ny,
@@ -555,6 +590,7 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
     h->seq_launches[seq] = launches;
     h->seq_pairs[seq] = pairs;
     h->seq_d[seq] = dsum;
+    h->seq_pruned[seq] = epi == EPI_CHUNK && args.alive != nullptr;
   }
   return pairs;
 }
@@ -663,7 +699,8 @@ std::vector<unsigned char> angle_graph_key(Ctx& c, const NormRun& r, int epi) {
                         (const void*)h->tspec.as<void>(), (const void*)h->ispec.as<void>(),
                         (const void*)h->Q.as<void>(), (const void*)h->gen_z.as<void>(),
                         (const void*)h->gen_x.as<void>(), (const void*)a.S1, (const void*)a.S2, (const void*)a.peak,
-                        (const void*)a.musig, (const void*)a.offx, (const void*)a.offy,
+                        (const void*)a.musig, (const void*)a.alive, (const void*)a.alive_win,
+                        (const void*)a.offx, (const void*)a.offy,
                         (const void*)a.cand, (const void*)a.cand_count, (const void*)h->dev_err.as<void>(),
                         (const void*)h->angle_table.as<void>(), (const void*)h->angle_cursor.as<void>(),
                         (const void*)h->angle_cur.as<void>()})
@@ -765,7 +802,9 @@ void run_angles(Ctx& c, NormRun& r, int epi, int a0, int a1) {
 
 // Sweep 1 (ComputeCCGSum norm.cu:523-544) or the single top-K sweep over angles [a0, a1).
 void norm_sweep1(Ctx& c, NormRun& r, int a0, int a1) {
-  run_angles(c, r, r.topk ? EPI_TOPK : EPI_SUM, a0, a1);
+  // with pruning the sums come with each pixel's best correlation (the top-K epilogue: the same
+  // sums, added in the same order)
+  run_angles(c, r, (r.topk || r.prune) ? EPI_TOPK : EPI_SUM, a0, a1);
   r.phase = 2;
 }
 
@@ -776,6 +815,18 @@ void norm_stats(Ctx& c, NormRun& r) {
                                                                     ms);
   GISSPA_LAUNCH_CHECK();
   r.args.musig = ms;
+  if (r.prune) {
+    const long long rows = (long long)r.W * c.l;
+    unsigned char* alive = buf<unsigned char>(c.h->alive, (size_t)rows + r.W);
+    unsigned* cnt = buf<unsigned>(c.h->alive_count, 1);
+    GISSPA_CUDA(cudaMemsetAsync(alive + rows, 0, r.W, c.s));
+    GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
+    row_alive_kernel<<<ceil_div(rows * 32, 256), 256, 0, c.s>>>(r.args.peak, ms, c.l, rows, r.args.thresh, alive,
+                                                               alive + rows, cnt);
+    GISSPA_LAUNCH_CHECK();
+    r.args.alive = alive;
+    r.args.alive_win = alive + rows;
+  }
   r.phase = 3;
 }
 
@@ -795,10 +846,14 @@ void norm_sweep2(Ctx& c, NormRun& r, int a0, int a1) {
     r.args.cand_cap = cap;
     run_angles(c, r, EPI_CHUNK, a0, a1);
     GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
-    unsigned count = 0;
+    unsigned count = 0, alive_rows = 0;
     GISSPA_CUDA(cudaMemcpyAsync(&count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c.s));
+    if (r.args.alive)
+      GISSPA_CUDA(cudaMemcpyAsync(&alive_rows, h->alive_count.as<unsigned>(), sizeof(unsigned),
+                                  cudaMemcpyDeviceToHost, c.s));
     GISSPA_CUDA(cudaStreamSynchronize(c.s));
     h->st.candidates = count;
+    h->st.rows_alive = r.args.alive ? (double)alive_rows / ((double)r.W * c.l) : 1.0;
     if (count > cap) {  // grow and repeat the second sweep only
       cap = count + count / 4 + 1024;
       continue;
@@ -910,6 +965,11 @@ void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_
   gisspa_handle* h = c.h;
   NormRun& r = h->run;
   norm_prepare(c, d_img, nx, ny, r);
+  r.prune = h->cfg.prune_sweep2 != 0 && !r.topk && correlate_fast(c.l);
+  if (r.prune) {  // sweep 1 keeps each pixel's best correlation
+    r.args.peak = buf<unsigned long long>(h->peak, r.npix);
+    GISSPA_CUDA(cudaMemsetAsync(r.args.peak, 0, sizeof(unsigned long long) * r.npix, c.s));
+  }
   const int A = (int)r.angles.size();
   norm_sweep1(c, r, 0, A);
   if (h->after_sweep1) {  // the sweep is queued: the host is free until the picks are read
@@ -1499,6 +1559,7 @@ void run_search(gisspa_handle* h, const float* d_img, int nx, int ny, const giss
   double tq = 0;
   long long nl = 0, np = 0, nd = 0;
   for (int i = 0; i < h->n_seqs; ++i) {
+    if (h->seq_pruned[i]) continue;  // the launch pair's time is that of full work
     float q = 0;
     GISSPA_CUDA(cudaEventElapsedTime(&q, h->qev[i][0], h->qev[i][1]));
     tq += q;
@@ -1658,6 +1719,9 @@ int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx
     total.pass_samples += h->st.pass_samples;
     total.graph_replays += h->st.graph_replays;
     total.window_size = h->st.window_size;
+    total.rows_alive += h->st.rows_alive / n;
+    total.pass_a_variant = h->st.pass_a_variant;
+    total.pass_b_variant = h->st.pass_b_variant;
     all.insert(all.end(), one.begin(), one.end());
     offsets[i + 1] = all.size();
   }

@@ -33,6 +33,7 @@ struct NormRun {
   std::vector<float> angles;
   double Ntot = 0;
   bool topk = false;
+  bool prune = false;  // sweep 2 skips the rows that cannot hold a pick (search_norm only)
   int D = 1, E = 1;
   CorrArgs args{};
   long long pairs = 0;
@@ -80,6 +81,7 @@ struct gisspa_handle {
   gisspa::DevBuf S1, S2, peak, musig;
   // correlation intermediate and outputs
   gisspa::DevBuf Q, cand, cand_count, nn_key, nn_sum, zkey, zcand, zcount;
+  gisspa::DevBuf alive, alive_count;  // rows sweep 2 transforms (prune_sweep2)
   gisspa::DevBuf engine_ctr;  // work counters of the pair engine, one block per launch of a sequence
   gisspa::DevBuf gen_z, gen_x;  // workspace of the generic correlation (window sizes without tuned kernels)
   gisspa::DevBuf dev_err;  // set by kernels whose bounded waits gave up
@@ -119,6 +121,7 @@ struct gisspa_handle {
   static constexpr int kSeqs = 16;
   cudaEvent_t qev[kSeqs][2] = {};
   long long seq_launches[kSeqs] = {}, seq_pairs[kSeqs] = {}, seq_d[kSeqs] = {};
+  bool seq_pruned[kSeqs] = {};  // a sweep-2 run that skipped rows: not the full work per pair
   int n_seqs = 0;
 
   ~gisspa_handle() {

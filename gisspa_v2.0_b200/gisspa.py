@@ -39,7 +39,8 @@ class Config(C.Structure):
                [("pick_mode", C.c_int), ("topk", C.c_int), ("exclusion_radius", C.c_float),
                 ("spectrum_precision", C.c_int), ("template_batch", C.c_int), ("window_batch", C.c_int),
                 ("quirks", C.c_int), ("tile_size", C.c_int), ("cuda_graphs", C.c_int), ("pass_b_shape", C.c_int),
-                ("tensor_cores", C.c_int), ("pass_a_shape", C.c_int)]
+                ("tensor_cores", C.c_int), ("pass_a_shape", C.c_int),
+                ("prune_sweep2", C.c_int)]
 
     @classmethod
     def default(cls, **kw) -> "Config":
@@ -55,6 +56,7 @@ class Config(C.Structure):
         c.quirks, c.tile_size, c.cuda_graphs, c.pass_b_shape = QUIRKS_REFERENCE, 720, 1, -1
         c.tensor_cores = 0
         c.pass_a_shape = -1
+        c.prune_sweep2 = 1
         for k, v in kw.items():
             if not hasattr(c, k):
                 raise KeyError(k)
@@ -105,7 +107,8 @@ class Stats(C.Structure):
                 ("pass_b_us", C.c_double), ("pairs_per_launch", C.c_double), ("templates_per_launch", C.c_double),
                 ("pass_samples", C.c_int), ("window_size", C.c_int), ("pass_b_variant", C.c_int),
                 ("tuned_us_per_pair", C.c_double), ("graph_replays", C.c_longlong), ("corr_pair_us", C.c_double),
-                ("corr_timed_launches", C.c_longlong), ("pass_a_variant", C.c_int)]
+                ("corr_timed_launches", C.c_longlong), ("pass_a_variant", C.c_int),
+                ("rows_alive", C.c_double)]
 
 
 class ShardInfo(C.Structure):

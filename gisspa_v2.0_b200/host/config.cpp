@@ -3,7 +3,8 @@
 // Same syntax: a stream of "key = value" tokens; unknown keys are ignored; keys
 // have the reference's types and defaults (DataReader2.h:19-44).  Extension keys
 // (pick_mode, topk, exclusion_radius, spectrum_precision, template_batch,
-// window_batch, quirks, tile_size, cuda_graphs, pass_b_shape, tensor_cores, pass_a_shape) configure the additions of
+// window_batch, quirks, tile_size, cuda_graphs, pass_b_shape, tensor_cores, pass_a_shape,
+// prune_sweep2) configure the additions of
 // this library.
 #include <cstdio>
 #include <cstring>
@@ -99,6 +100,7 @@ extern "C" int gisspa_config_load(const char* path, gisspa_config* cfg, gisspa_r
     else if (key == "pass_b_shape") ok = parse_int(val, cfg->pass_b_shape);
     else if (key == "tensor_cores") ok = parse_int(val, cfg->tensor_cores);
     else if (key == "pass_a_shape") ok = parse_int(val, cfg->pass_a_shape);
+    else if (key == "prune_sweep2") ok = parse_int(val, cfg->prune_sweep2);
     // unknown keys are ignored (DataReader2.cpp:17-18)
     if (!ok) return GISSPA_ERR_IO;
   }

@@ -89,6 +89,11 @@ typedef struct gisspa_config {
   int pass_a_shape;       /* with template_batch and window_batch set: column-transform kernel shape
                              (0 .. compiled shapes - 1: two at window 512, one elsewhere; -1 = the
                              first); ignored when autotuning */
+  int prune_sweep2;       /* norm_type=1 chunk picks at window sizes with hand-tuned kernels: 1
+                             (default) = sweep 1 also keeps each pixel's best correlation, and
+                             sweep 2 skips the window rows whose best z is below the threshold
+                             (they cannot hold a pick for any template or angle: same picks);
+                             0 = sweep 2 transforms every row */
 } gisspa_config;
 
 /* Per-micrograph CTF, as in an LST line "defocus= dfdiff= dfang=" (DataReader2.h:93-103).
@@ -142,10 +147,14 @@ typedef struct gisspa_stats {
   double tuned_us_per_pair;    /* autotuner's measured time per pair of that shape */
   long long graph_replays;     /* angles run as replays of a captured CUDA graph */
   /* CUDA events around whole runs of correlation launches (every host-launched angle: the
-   * first of each sweep when graphs are on), nothing recorded between them */
+   * first of each sweep when graphs are on, except a pruned second sweep), nothing recorded
+   * between them */
   double corr_pair_us;         /* mean duration of one pass A + pass B launch pair */
   long long corr_timed_launches; /* launch pairs inside those runs */
   int pass_a_variant;          /* pass A shape picked by the autotuner (last sweep) */
+  double rows_alive;           /* fraction of window rows sweep 2 transformed (below 1 with
+                                  prune_sweep2; 0 when the search has no second sweep; a batch
+                                  reports the mean over its micrographs) */
 } gisspa_stats;
 
 typedef struct gisspa_handle gisspa_handle;

@@ -283,3 +283,27 @@ def test_pair_engine_bit_identical_to_per_pass_kernels(mode, graphs):
     assert np.array_equal(g0, g4)
     if mode == "chunk":
         assert np.array_equal(ms0, ms4)
+
+
+@pytest.mark.parametrize("raise_threshold", [0.0, 2.0])
+@pytest.mark.parametrize("name", ["norm_l256_w9", "norm_l512_w4", "norm_l1024_w4", "norm_l320_w4"])
+def test_pruned_second_sweep_gives_the_same_picks(name, raise_threshold):
+    """Sweep 2 with the rows that cannot hold a pick skipped (prune_sweep2 = 1, the default)
+    against sweep 2 over every row: the same chunk picks bit for bit (none, for some cases, at
+    the raised threshold, where rows are skipped).  (Fixed launch shapes: the autotuner may pick another column-transform shape
+    for either search, whose rounding differs in the last bits.)"""
+    img, tmpl, ctf, cfg = small_case(name)
+    cfg = cfg.copy(threshold=cfg.threshold + raise_threshold, template_batch=2, window_batch=2, pass_a_shape=0,
+                   pass_b_shape=0)
+    res = []
+    for prune in (0, 1):
+        s = gisspa.Searcher(cfg.copy(prune_sweep2=prune))
+        s.set_templates(tmpl)
+        g = s.search(img, ctf)
+        res.append((g, s.stats().rows_alive))
+        s.close()
+    (g0, r0), (g1, r1) = res
+    assert (len(g0) > 0 or raise_threshold) and np.array_equal(g0, g1)
+    assert r0 == 1.0 and 0.0 <= r1 <= 1.0
+    if raise_threshold:
+        assert r1 < 1.0
