@@ -99,21 +99,22 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   // per-pixel sums as pairs (pixels 2j, 2j + 1 of output element j): one paired FP32
   // instruction adds a row's two values, with the rounding of two scalar additions
   float2 acc1[RPT][E], acc2[RPT][E];
-  float best[(EPI == EPI_TOPK) ? RPT : 1][E][2];
+  constexpr bool SUMS = EPI == EPI_SUM || EPI == EPI_TOPK || EPI == EPI_SUMMAX;
+  float best[(EPI == EPI_TOPK || EPI == EPI_SUMMAX) ? RPT : 1][E][2];
   int barg[(EPI == EPI_TOPK) ? RPT : 1][E][2];
   float2 mu[(EPI == EPI_CHUNK) ? RPT : 1][E], isg[(EPI == EPI_CHUNK) ? RPT : 1][E];
-  if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+  if constexpr (SUMS) {
 #pragma unroll
     for (int s = 0; s < RPT; ++s)
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         acc1[s][i] = make_float2(0.f, 0.f);
         acc2[s][i] = make_float2(0.f, 0.f);
-        if constexpr (EPI == EPI_TOPK) {
+        if constexpr (EPI == EPI_TOPK || EPI == EPI_SUMMAX) {
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             best[s][i][h] = -INFINITY;
-            barg[s][i][h] = -1;
+            if constexpr (EPI == EPI_TOPK) barg[s][i][h] = -1;
           }
         }
       }
@@ -165,12 +166,16 @@ __global__ void __launch_bounds__(NW * 32, MINB)
       const TeamSync<TEAM> tsync{1 + team};
       RX::run(v, row, tw_nz, tw_l, lt, tsync);
 
-      if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+      if constexpr (SUMS) {
 #pragma unroll
         for (int i = 0; i < E; ++i) {
           // raw values: the 1/L^2 is applied when folding
           acc1[s][i] = cadd(acc1[s][i], v[i]);
           acc2[s][i] = pfma(v[i], v[i], acc2[s][i]);
+          if constexpr (EPI == EPI_SUMMAX) {
+            best[s][i][0] = fmaxf(best[s][i][0], v[i].x);
+            best[s][i][1] = fmaxf(best[s][i][1], v[i].y);
+          }
           if constexpr (EPI == EPI_TOPK) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -327,7 +332,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   // return nothing, so no warp waits on the state's memory latency.  Each pixel receives one
   // reduction per launch and launches are stream-ordered: the additions happen in the same
   // order, with the same rounding, as a read-modify-write.
-  if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+  if constexpr (SUMS) {
 #pragma unroll
     for (int s = 0; s < RPT; ++s) {
       const int oy = (y0 + team + NTEAM * s + L / 2) % L;
@@ -343,6 +348,8 @@ __global__ void __launch_bounds__(NW * 32, MINB)
               atomicMax(a.peak + pix + h, ((unsigned long long)float_key(best[s][i][h] * inv) << 32) |
                                               (unsigned)(0xFFFFFFFFu - (unsigned)barg[s][i][h]));
           }
+          if constexpr (EPI == EPI_SUMMAX)
+            atomicMax(a.peak + pix + h, (unsigned long long)float_key(best[s][i][h] * inv) << 32);
         }
       }
     }
@@ -440,6 +447,7 @@ void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, con
   if constexpr (P::TEAM > 32) {
     switch (cl.epi) {
       case EPI_SUM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_SUM, P::MINB>(cl, args, twL, twNZ, s); break;
+      case EPI_SUMMAX: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_SUMMAX, P::MINB>(cl, args, twL, twNZ, s); break;
       case EPI_TOPK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_TOPK, P::MINB>(cl, args, twL, twNZ, s); break;
       case EPI_CHUNK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_CHUNK, P::MINB>(cl, args, twL, twNZ, s); break;
       case EPI_MAP: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_MAP, P::MINB>(cl, args, twL, twNZ, s); break;
@@ -449,6 +457,7 @@ void launch_b(const CorrLaunch& cl, const CorrArgs& args, const float2* twL, con
   } else {
   switch (cl.epi) {
     case EPI_SUM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_SUM, P::MINB>(cl, args, twL, twNZ, s); break;
+    case EPI_SUMMAX: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_SUMMAX, P::MINB>(cl, args, twL, twNZ, s); break;
     case EPI_CHUNK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_CHUNK, P::MINB>(cl, args, twL, twNZ, s); break;
     case EPI_TOPK: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_TOPK, P::MINB>(cl, args, twL, twNZ, s); break;
     case EPI_NONORM: launch_b_cfg<L, P::TEAM, P::RB, P::NW, EPI_NONORM, P::MINB>(cl, args, twL, twNZ, s); break;
@@ -526,7 +535,7 @@ bool correlate_variant_ok(int L, int variant, int epi) {
   if (variant < 0 || variant >= correlate_variants(L)) return false;
   if (variant == engine_variant(L)) return engine_supported(L, epi);
   const bool wide = L == 1024 && variant >= 3;  // 64-lane rows
-  return !wide || epi == EPI_SUM || epi == EPI_TOPK || epi == EPI_CHUNK || epi == EPI_MAP;
+  return !wide || epi == EPI_SUM || epi == EPI_SUMMAX || epi == EPI_TOPK || epi == EPI_CHUNK || epi == EPI_MAP;
 }
 
 int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,

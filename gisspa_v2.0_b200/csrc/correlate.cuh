@@ -23,7 +23,8 @@ enum Epilogue : int {
   EPI_CHUNK = 1,   // sweep 2: z = (c - mu) / sigma, 256-pixel chunk max, threshold -> candidates
   EPI_TOPK = 2,    // one sweep: S1, S2 and per-pixel max c with its (angle, template)
   EPI_NONORM = 3,  // norm_type=0: per pair peak (border zeroed), sum, sum of squares of CC
-  EPI_MAP = 4      // write c maps (tests and the no-scratch entry point)
+  EPI_MAP = 4,     // write c maps (tests and the no-scratch entry point)
+  EPI_SUMMAX = 5   // sweep 1 of a pruned search: S1, S2 and the per-pixel max c (peak key, no index)
 };
 
 // A picked chunk (or, for EPI_NONORM, nothing: per-pair reductions go to nn_*).
@@ -97,7 +98,7 @@ int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float
 
 // The pair engine (pair_engine.cu): one launch runs pass A of one batch and pass B of the batch
 // before it, so that the load-bound and the issue-bound pass share the SMs.  Window 512, epilogues
-// EPI_SUM, EPI_TOPK and EPI_CHUNK.
+// EPI_SUM, EPI_SUMMAX, EPI_TOPK and EPI_CHUNK.
 struct EngineBatch {
   int valid;          // 0: no such pass in this launch
   int b0, n0, d, e;   // first window, first template, templates, windows

@@ -10,7 +10,7 @@
 // (the first only pass A, the last only pass B); the outputs, their order and rounding are those
 // of the per-pass kernels (correlate.cu): the same device code computes every value.
 //
-// Window 512 only, epilogues EPI_SUM, EPI_TOPK and EPI_CHUNK.  Pass B runs one warp per row (the
+// Window 512 only, epilogues EPI_SUM, EPI_SUMMAX, EPI_TOPK and EPI_CHUNK.  Pass B runs one warp per row (the
 // per-pass kernel's 32-lane team), each warp with its own double-buffered stage of Q rows filled
 // by bulk copies, so B rows need no CTA-wide barrier.
 #include "../../include/gisspa.h"
@@ -62,19 +62,20 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
   for (int i = 0; i < E; ++i) ox[i] = (2 * RX::out_index(lane, i) + kL / 2) % kL;
 
   float2 acc1[E], acc2[E];  // pixels 2j, 2j + 1 of output element j as pairs
-  float best[(EPI == EPI_TOPK) ? E : 1][2];
+  constexpr bool SUMS = EPI == EPI_SUM || EPI == EPI_TOPK || EPI == EPI_SUMMAX;
+  float best[(EPI == EPI_TOPK || EPI == EPI_SUMMAX) ? E : 1][2];
   int barg[(EPI == EPI_TOPK) ? E : 1][2];
   float2 mu[(EPI == EPI_CHUNK) ? E : 1], isg[(EPI == EPI_CHUNK) ? E : 1];
-  if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+  if constexpr (SUMS) {
 #pragma unroll
     for (int i = 0; i < E; ++i) {
       acc1[i] = make_float2(0.f, 0.f);
       acc2[i] = make_float2(0.f, 0.f);
-      if constexpr (EPI == EPI_TOPK) {
+      if constexpr (EPI == EPI_TOPK || EPI == EPI_SUMMAX) {
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           best[i][h] = -INFINITY;
-          barg[i][h] = -1;
+          if constexpr (EPI == EPI_TOPK) barg[i][h] = -1;
         }
       }
     }
@@ -121,11 +122,15 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
     float2 v[RX::EBUF];
     RX::run(v, stage + (d & 1) * kNZ, tw_nz, tw_l, lane, WarpSync{});
 
-    if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+    if constexpr (SUMS) {
 #pragma unroll
       for (int i = 0; i < E; ++i) {
         acc1[i] = cadd(acc1[i], v[i]);  // raw: the 1/L^2 is applied when folding
         acc2[i] = pfma(v[i], v[i], acc2[i]);
+        if constexpr (EPI == EPI_SUMMAX) {
+          best[i][0] = fmaxf(best[i][0], v[i].x);
+          best[i][1] = fmaxf(best[i][1], v[i].y);
+        }
         if constexpr (EPI == EPI_TOPK) {
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
@@ -171,7 +176,7 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
     __syncwarp();  // this stage buffer is refilled two templates later
   }
 
-  if constexpr (EPI == EPI_SUM || EPI == EPI_TOPK) {
+  if constexpr (SUMS) {
 #pragma unroll
     for (int i = 0; i < E; ++i) {
       const size_t pix = wbase + (size_t)oy * kL + ox[i];
@@ -184,6 +189,8 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
             atomicMax(a.peak + pix + h, ((unsigned long long)float_key(best[i][h] * inv) << 32) |
                                             (unsigned)(0xFFFFFFFFu - (unsigned)barg[i][h]));
         }
+        if constexpr (EPI == EPI_SUMMAX)
+          atomicMax(a.peak + pix + h, (unsigned long long)float_key(best[i][h] * inv) << 32);
       }
     }
   }
@@ -286,6 +293,7 @@ template <typename SPEC>
 void launch_spec(int epi, const EngineArgs& g, cudaStream_t s) {
   switch (epi) {
     case EPI_SUM: launch_cfg<SPEC, EPI_SUM>(g, s); break;
+    case EPI_SUMMAX: launch_cfg<SPEC, EPI_SUMMAX>(g, s); break;
     case EPI_TOPK: launch_cfg<SPEC, EPI_TOPK>(g, s); break;
     case EPI_CHUNK: launch_cfg<SPEC, EPI_CHUNK>(g, s); break;
     default: throw CudaError{cudaErrorInvalidValue, "pair engine without this epilogue"};
@@ -294,7 +302,9 @@ void launch_spec(int epi, const EngineArgs& g, cudaStream_t s) {
 
 }  // namespace
 
-bool engine_supported(int L, int epi) { return L == kL && (epi == EPI_SUM || epi == EPI_TOPK || epi == EPI_CHUNK); }
+bool engine_supported(int L, int epi) {
+  return L == kL && (epi == EPI_SUM || epi == EPI_SUMMAX || epi == EPI_TOPK || epi == EPI_CHUNK);
+}
 
 size_t engine_counter_ints() { return 2 + kSmSlots; }
 

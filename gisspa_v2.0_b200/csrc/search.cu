@@ -99,7 +99,8 @@ int validate_config(const gisspa_config& c, std::string& err) {
     return GISSPA_ERR_ARG;
   }
   if (c.pass_b_shape >= 0) {
-    const int epis[3] = {c.norm_type == 0 ? EPI_NONORM : (c.pick_mode == GISSPA_PICK_TOPK ? EPI_TOPK : EPI_SUM),
+    const int sweep1 = c.pick_mode == GISSPA_PICK_TOPK ? EPI_TOPK : c.prune_sweep2 ? EPI_SUMMAX : EPI_SUM;
+    const int epis[3] = {c.norm_type == 0 ? EPI_NONORM : sweep1,
                          c.norm_type == 0 ? EPI_NONORM : EPI_CHUNK, EPI_MAP};
     for (int k = 0; k < (c.norm_type != 0 && c.pick_mode == GISSPA_PICK_CHUNK ? 2 : 1); ++k)
       if (!correlate_variant_ok(l, c.pass_b_shape, epis[k])) {
@@ -488,7 +489,7 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
         };
         at(0);
         GISSPA_CUDA(cudaEventRecord(h->ev[5], c.s));
-        constexpr int kReps = 3;
+        constexpr int kReps = 6;
         for (int r = 1; r <= kReps; ++r) at(r);
         GISSPA_CUDA(cudaEventRecord(h->ev[6], c.s));
         GISSPA_CUDA(cudaEventSynchronize(h->ev[6]));
@@ -802,9 +803,9 @@ void run_angles(Ctx& c, NormRun& r, int epi, int a0, int a1) {
 
 // Sweep 1 (ComputeCCGSum norm.cu:523-544) or the single top-K sweep over angles [a0, a1).
 void norm_sweep1(Ctx& c, NormRun& r, int a0, int a1) {
-  // with pruning the sums come with each pixel's best correlation (the top-K epilogue: the same
-  // sums, added in the same order)
-  run_angles(c, r, (r.topk || r.prune) ? EPI_TOPK : EPI_SUM, a0, a1);
+  // with pruning the sums come with each pixel's best correlation (the same sums, added in the
+  // same order)
+  run_angles(c, r, r.topk ? EPI_TOPK : r.prune ? EPI_SUMMAX : EPI_SUM, a0, a1);
   r.phase = 2;
 }
 
