@@ -681,6 +681,7 @@ def main():
                             "sweep2": stats[-1].ms_sweep2, "pick": stats[-1].ms_pick},
                "gpu_launches": int(launches), "graph_replays": int(stats[-1].graph_replays), "clocks": clk,
                "roofline": roofline, "e2e": e2e, "rows_alive": float(stats[-1].rows_alive),
+               "pairs_alive": float(stats[-1].pairs_alive),
                "plain_full_sweeps": full}
         if chosen is not None:
             res["chosen_form"] = chosen

@@ -79,8 +79,7 @@ template <int L, typename SPEC, int V = 0>
 __device__ __forceinline__ void pass_a_body(float2* smem, const float2* __restrict__ I,
                                             const typename SPEC::T* __restrict__ T, float2* __restrict__ Q, int b0,
                                             int n0, int D, const float2* __restrict__ twL, int p, int cgroup,
-                                            bool wait_before_store, const unsigned char* __restrict__ alive,
-                                            const unsigned char* __restrict__ alive_win) {
+                                            bool wait_before_store, const SkipMask& sk) {
   constexpr int TT = PassA<L, V>::TT, NC = PassA<L, V>::NC, E = L / TT, NZ = L / 2, HS = NZ + 1;
   using CX = ColXform<L, TT>;
   constexpr int SH = NC >= 16 ? 0 : NC == 8 ? 1 : 2;
@@ -89,7 +88,7 @@ __device__ __forceinline__ void pass_a_body(float2* smem, const float2* __restri
   const int team = threadIdx.x / TT, tid = threadIdx.x - team * TT;
   const int c0 = cgroup * NC, c = c0 + team;
   const int e = p / D, d = p - e * D;
-  if (alive_win && !alive_win[b0 + e]) {  // no row of this window is needed (CTA-uniform)
+  if ((sk.windows && !sk.windows[b0 + e]) || !sk.pair_live(b0 + e, n0 + d)) {  // nothing needed (CTA-uniform)
     if (wait_before_store) griddep_wait();  // complete only after the kernel before, as when storing
     return;
   }
@@ -127,7 +126,7 @@ __device__ __forceinline__ void pass_a_body(float2* smem, const float2* __restri
   constexpr int HALF = NC / 2;  // 16-byte pairs per row segment
   // (a runtime loop: unrolled, with the swizzle at 16-byte granularity so that no pair needs
   // its halves swapped, the launch pair measured 75.0 against 69.9 us at window 512)
-  const unsigned char* live = alive ? alive + (size_t)(b0 + e) * L : nullptr;
+  const unsigned char* live = sk.rows ? sk.rows + (size_t)(b0 + e) * L : nullptr;
   for (int u = threadIdx.x; u < L * HALF; u += TT * NC) {
     const int y = u / HALF, k = (u - y * HALF) * 2, sw = (y >> SH) & (NC - 1);
     if (live && !live[y]) continue;  // a row the next pass skips
@@ -145,6 +144,13 @@ __device__ __forceinline__ unsigned long long team_max_u64(unsigned long long k)
     k = o > k ? o : k;
   }
   return k;
+}
+// Maximum over each group of W lanes (a power of two up to 32) of the warp.
+template <int W>
+__device__ __forceinline__ float group_max(float x) {
+#pragma unroll
+  for (int off = W / 2; off > 0; off >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, off, W));
+  return x;
 }
 template <int TEAM>
 __device__ __forceinline__ double team_sum_f64(double x) {

@@ -12,12 +12,32 @@ namespace {
 template <int L, typename SPEC, int V>
 __global__ void __launch_bounds__(PassA<L, V>::TT * PassA<L, V>::NC, PassA<L, V>::MINB)
     pass_a_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
-                  int b0, int n0, int D, const float2* __restrict__ twL, int chained,
-                  const unsigned char* __restrict__ alive, const unsigned char* __restrict__ alive_win) {
+                  int b0, int n0, int D, const float2* __restrict__ twL, int chained, SkipMask sk) {
   extern __shared__ __align__(16) float2 smem[];  // [NC * L]: FFT exchange buffers, then the output tile
   griddep_launch_dependents();
   if (!chained) griddep_wait();  // the spectra may come from the kernel just before
-  pass_a_body<L, SPEC, V>(smem, I, T, Q, b0, n0, D, twL, blockIdx.y, blockIdx.x, chained != 0, alive, alive_win);
+  pass_a_body<L, SPEC, V>(smem, I, T, Q, b0, n0, D, twL, blockIdx.y, blockIdx.x, chained != 0, sk);
+}
+
+// Pass A of a pruned second sweep: one CTA per pair looping over the column groups, so that the
+// (almost all) dead pairs cost one CTA each instead of one per column group.
+template <int L, typename SPEC, int V>
+__global__ void __launch_bounds__(PassA<L, V>::TT * PassA<L, V>::NC, PassA<L, V>::MINB)
+    pass_a_pair_kernel(const float2* __restrict__ I, const typename SPEC::T* __restrict__ T, float2* __restrict__ Q,
+                       int b0, int n0, int D, const float2* __restrict__ twL, int chained, SkipMask sk) {
+  extern __shared__ __align__(16) float2 smem[];
+  constexpr int NZ = L / 2, NC = PassA<L, V>::NC;
+  griddep_launch_dependents();
+  if (!chained) griddep_wait();
+  const int p = blockIdx.x, e = p / D, d = p - e * D;
+  if ((sk.windows && !sk.windows[b0 + e]) || !sk.pair_live(b0 + e, n0 + d)) {
+    if (chained) griddep_wait();  // complete only after the kernel before, as when storing
+    return;
+  }
+  for (int cg = 0; cg < NZ / NC; ++cg) {
+    if (cg) __syncthreads();  // the previous group's output tile has been read
+    pass_a_body<L, SPEC, V>(smem, I, T, Q, b0, n0, D, twL, p, cg, chained != 0, sk);
+  }
 }
 
 // Pass B: a team (TEAM lanes) per output row; RB rows per CTA, one window per blockIdx.y,
@@ -48,9 +68,9 @@ __global__ void __launch_bounds__(NW * 32, MINB)
   if constexpr (EPI == EPI_CHUNK) {
     // rows that cannot hold a pick are skipped; a CTA with none left leaves at once, after the
     // pass A before it has completed (so that this kernel completes after it, as when it reads Q)
-    if (a.alive) {
+    if (a.skip.rows) {
       bool any = false;
-      for (int r = 0; r < RB; ++r) any = any || a.alive[(size_t)win * L + y0 + r] != 0;
+      for (int r = 0; r < RB; ++r) any = any || a.skip.rows[(size_t)win * L + y0 + r] != 0;
       if (!any) {
         griddep_wait();
         return;
@@ -80,14 +100,41 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     mbar_init(&bars[1], 1);
     fence_mbar_init();
   }
+  // the launch's templates this CTA transforms: all of them, or for a pruned second sweep those
+  // whose pair with this window is live (pass A stored no Q for the others)
+  __shared__ unsigned char live_d[EPI == EPI_CHUNK ? kMaxListedTemplates : 1];
+  __shared__ int n_live;
+  int nd = a.D;
+  bool listed = false;
+  if constexpr (EPI == EPI_CHUNK) {
+    listed = a.skip.pairs != nullptr && a.D <= kMaxListedTemplates;
+    if (listed) {
+      for (int d = threadIdx.x; d < a.D; d += NW * 32) live_d[d] = a.skip.pair_live(win, a.n0 + d) ? 1 : 0;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int n = 0;
+        for (int d = 0; d < a.D; ++d)
+          if (live_d[d]) live_d[n++] = (unsigned char)d;
+        n_live = n;
+      }
+    }
+  }
   __syncthreads();
+  if (listed) {
+    nd = n_live;
+    if (nd == 0) {  // (CTA-uniform) as for dead rows above
+      griddep_wait();
+      return;
+    }
+  }
+  auto dof = [&](int k) { return listed ? (int)live_d[k] : k; };
   griddep_launch_dependents();
   griddep_wait();  // Q comes from the pass A just before
-  auto issue = [&](int d) {
-    const float2* src = a.Q + ((size_t)(e * a.D + d) * L + y0) * NZ;
+  auto issue = [&](int k) {
+    const float2* src = a.Q + ((size_t)(e * a.D + dof(k)) * L + y0) * NZ;
     fence_proxy_async_smem();
-    mbar_expect_tx(&bars[d & 1], kStageBytes);
-    bulk_g2s(stage + (d & 1) * RB * NZ, src, kStageBytes, &bars[d & 1]);
+    mbar_expect_tx(&bars[k & 1], kStageBytes);
+    bulk_g2s(stage + (k & 1) * RB * NZ, src, kStageBytes, &bars[k & 1]);
   };
   if (threadIdx.x == 0) issue(0);
 
@@ -133,24 +180,28 @@ __global__ void __launch_bounds__(NW * 32, MINB)
     }
   }
 
+  __shared__ unsigned pmax_s[2];  // EPI_SUMMAX: the pair maximum of templates k, k + 1
+  if (EPI == EPI_SUMMAX && threadIdx.x < 2) pmax_s[threadIdx.x] = 0u;
+  __syncthreads();
   int issued = 1;
-  for (int d = 0; d < a.D; ++d) {
+  for (int k = 0; k < nd; ++k) {
+    const int d = dof(k);
     const int p = e * a.D + d;
-    if (threadIdx.x == 0 && d + 1 < a.D) {
-      issue(d + 1);
+    if (threadIdx.x == 0 && k + 1 < nd) {
+      issue(k + 1);
       ++issued;
     }
-    const bool ok = mbar_wait(&bars[d & 1], (d >> 1) & 1, 4000000000LL);
+    const bool ok = mbar_wait(&bars[k & 1], (k >> 1) & 1, 4000000000LL);
     if (!__syncthreads_and(ok)) {
       if (threadIdx.x == 0) {
         atomicOr(a.err, 1u);
         // let copies already in flight land before the CTA's shared memory goes away
-        for (int k = d; k < issued; ++k) mbar_wait(&bars[k & 1], (k >> 1) & 1, 400000000LL);
+        for (int j = k; j < issued; ++j) mbar_wait(&bars[j & 1], (j >> 1) & 1, 400000000LL);
       }
       __syncthreads();
       return;
     }
-    float2* stg = stage + (d & 1) * RB * NZ;
+    float2* stg = stage + (k & 1) * RB * NZ;
     double nn_s1 = 0.0, nn_s2 = 0.0;
 #pragma unroll
     for (int s = 0; s < RPT; ++s) {
@@ -158,7 +209,7 @@ __global__ void __launch_bounds__(NW * 32, MINB)
       const int oy = (y0 + r + L / 2) % L;
       // a dead row (pass A did not store it) is skipped by its team; half-warp teams stay in
       // step (the chunk vote uses the whole warp): they transform it and discard its values
-      const bool row_live = EPI != EPI_CHUNK || !a.alive || a.alive[(size_t)win * L + y0 + r];
+      const bool row_live = EPI != EPI_CHUNK || !a.skip.rows || a.skip.rows[(size_t)win * L + y0 + r];
       if constexpr (EPI == EPI_CHUNK && TEAM >= 32)
         if (!row_live) continue;
       float2* row = stg + r * NZ;
@@ -185,6 +236,17 @@ __global__ void __launch_bounds__(NW * 32, MINB)
                 barg[s][i][h] = angle * a.nt_total + a.n0 + d;
               }
             }
+          }
+        }
+        if constexpr (EPI == EPI_SUMMAX) {
+          // the pair's maximum over the window: this row's, reduced over the team (or warp) and
+          // the CTA's rows in shared memory, and sent once per template (below)
+          if (a.pair_max) {
+            float m = -INFINITY;
+#pragma unroll
+            for (int i = 0; i < E; ++i) m = fmaxf(m, fmaxf(v[i].x, v[i].y));
+            m = group_max<(TEAM < 32 ? TEAM : 32)>(m);
+            if ((lt & 31) == 0) atomicMax(&pmax_s[k & 1], float_key(m * inv));
           }
         }
       } else if constexpr (EPI == EPI_CHUNK) {
@@ -326,6 +388,13 @@ __global__ void __launch_bounds__(NW * 32, MINB)
       }
     }
     __syncthreads();  // this stage buffer is refilled two templates later
+    if constexpr (EPI == EPI_SUMMAX) {
+      // every team's row maximum of template d is in (the next template uses the other slot)
+      if (threadIdx.x == 0 && a.pair_max) {
+        atomicMax(a.pair_max + pair_index(win, a.n0 + d, angle, a.n_windows, a.n_angles), pmax_s[k & 1]);
+        pmax_s[k & 1] = 0u;
+      }
+    }
   }
 
   // Fold this launch's partial sums (and maxima) into the per-pixel state with reductions that
@@ -374,6 +443,13 @@ void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaSt
   ++launch_counter();
 }
 
+// Pass A's mask: pairs only where pass B lists the live templates (D small enough).
+SkipMask a_mask(const CorrLaunch& cl, const CorrArgs& args) {
+  SkipMask m = args.skip;
+  if (cl.D > kMaxListedTemplates) m.pairs = nullptr;
+  return m;
+}
+
 template <int L, typename SPEC, int V>
 void launch_a_cfg(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
                   const float2* twL, cudaStream_t s) {
@@ -385,10 +461,20 @@ void launch_a_cfg(const CorrLaunch& cl, const float2* I, const void* T, float2* 
     GISSPA_CUDA(
         cudaFuncSetAttribute(pass_a_kernel<L, SPEC, V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   });
+  const SkipMask sk = cl.epi == EPI_CHUNK ? a_mask(cl, args) : SkipMask{};
+  if (sk.pairs) {
+    static PerDeviceOnce once_pair;
+    once_pair([] {
+      GISSPA_CUDA(cudaFuncSetAttribute(pass_a_pair_kernel<L, SPEC, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    });
+    launch_pdl(pass_a_pair_kernel<L, SPEC, V>, dim3(cl.E * cl.D), dim3(P::TT * P::NC), smem, s, I,
+               static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0, sk);
+    return;
+  }
   dim3 grid(NZ / P::NC, cl.E * cl.D);
   launch_pdl(pass_a_kernel<L, SPEC, V>, grid, dim3(P::TT * P::NC), smem, s, I,
-             static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0,
-             cl.epi == EPI_CHUNK ? args.alive : nullptr, cl.epi == EPI_CHUNK ? args.alive_win : nullptr);
+             static_cast<const typename SPEC::T*>(T), Q, args.b0, args.n0, cl.D, twL, cl.chained ? 1 : 0, sk);
 }
 template <int L, typename SPEC>
 void launch_a(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
@@ -538,8 +624,11 @@ bool correlate_variant_ok(int L, int variant, int epi) {
   return !wide || epi == EPI_SUM || epi == EPI_SUMMAX || epi == EPI_TOPK || epi == EPI_CHUNK || epi == EPI_MAP;
 }
 
-int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args,
+int correlate_launch(const CorrLaunch& cl, const float2* I, const void* T, float2* Q, const CorrArgs& args_in,
                      const float2* twL, const float2* twNZ, cudaStream_t s, cudaEvent_t* ev) {
+  CorrArgs args = args_in;
+  args.skip.angle = args.angle;
+  args.skip.angle_state = args.angle_state;
   switch (cl.L) {
     case 256: return launch_pair<256>(cl, I, T, Q, args, twL, twNZ, s, ev);
     case 320: return launch_pair<320>(cl, I, T, Q, args, twL, twNZ, s, ev);

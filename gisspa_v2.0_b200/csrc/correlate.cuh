@@ -35,6 +35,33 @@ struct Cand {
   int pad;
 };
 
+// Index of the (window, template, angle) pair in the per-pair arrays of a pruned search,
+// template-major: the pairs of one launch (a few windows and consecutive templates at one angle)
+// fall in different cache lines, and so in different L2 slices, for their atomic maxima.
+__host__ __device__ __forceinline__ size_t pair_index(int win, int templ, int angle, int n_windows, int n_angles) {
+  return ((size_t)templ * n_windows + win) * n_angles + angle;
+}
+
+// What the second sweep of a pruned search skips (null pointers: nothing).  Every pair's z at a
+// pixel is at most the z of the pixel's best correlation over all pairs, and a pair's correlation
+// is at most its maximum over the window: rows whose pixels cannot reach the threshold, windows
+// without such rows and pairs whose maximum stays below every live pixel's bar hold no pick.
+struct SkipMask {
+  const unsigned char* rows;     // [W][L] by row y of Q (output row (y + L/2) mod L)
+  const unsigned char* windows;  // [W]
+  const unsigned char* pairs;    // [nt_total][W][n_angles] (pair_index)
+  int nt_total, n_windows, n_angles;
+  int angle;                      // the launch's angle (set by correlate_launch)
+  const AngleState* angle_state;  // when set, the angle index is read here (graph replays)
+  __device__ __forceinline__ bool pair_live(int win, int templ) const {
+    if (!pairs) return true;
+    const int a = angle_state ? angle_state->index : angle;
+    return pairs[pair_index(win, templ, a, n_windows, n_angles)] != 0;
+  }
+};
+// Pair masks apply to launches of at most this many templates (pass B lists the live ones).
+constexpr int kMaxListedTemplates = 256;
+
 struct CorrArgs {
   const float2* Q;          // pass A output, row-major [pairs][L][L/2] (slot 0 packs columns 0 and L/2)
   unsigned* err;            // set to 1 when a bounded wait gives up
@@ -61,10 +88,13 @@ struct CorrArgs {
   Cand* cand;
   unsigned* cand_count;
   unsigned cand_cap;
-  // EPI_CHUNK (optional): the window rows that can still hold a pick, alive[window][y] by row of
-  // Q (output row (y + L/2) mod L), and alive_win[window]; rows and windows marked 0 are skipped
-  const unsigned char* alive;
-  const unsigned char* alive_win;
+  // EPI_CHUNK (optional): rows, windows and pairs that are skipped (their nt_total, n_angles,
+  // angle and angle_state are those of the launch)
+  SkipMask skip;
+  // EPI_SUMMAX (optional): each (window, template, angle) pair's maximum correlation over the
+  // window, float_key(c) at pair_index(window, template, angle, n_windows, n_angles)
+  unsigned* pair_max;
+  int n_windows, n_angles;
   // EPI_NONORM, indexed [window][template] with nt_total templates per window
   unsigned long long* nn_key;
   double* nn_sum;           // [W][nt_total][2]

@@ -52,7 +52,7 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
   constexpr int E = RX::EOUT;
   const int win = a.b0 + e;
   if constexpr (EPI == EPI_CHUNK)
-    if (a.alive && !a.alive[(size_t)win * kL + y]) return true;  // a row that cannot hold a pick
+    if (a.skip.rows && !a.skip.rows[(size_t)win * kL + y]) return true;  // a row that cannot hold a pick
   const int angle = a.angle_state ? a.angle_state->index : a.angle;
   const int oy = (y + kL / 2) % kL;
   const float inv = 1.0f / (float)(kL * kL);
@@ -142,6 +142,16 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
           }
         }
       }
+      if constexpr (EPI == EPI_SUMMAX) {
+        if (a.pair_max) {  // the pair's maximum over the window, this row's part
+          float m = -INFINITY;
+#pragma unroll
+          for (int i = 0; i < E; ++i) m = fmaxf(m, fmaxf(v[i].x, v[i].y));
+          m = group_max<32>(m);
+          if (lane == 0)
+            atomicMax(a.pair_max + pair_index(win, a.n0 + d, angle, a.n_windows, a.n_angles), float_key(m * inv));
+        }
+      }
     } else if constexpr (EPI == EPI_CHUNK) {
       constexpr int CPR = kL / 256;
       const int c0 = (oy * kL) >> 8;
@@ -197,6 +207,18 @@ __device__ __forceinline__ bool engine_row(const CorrArgs& a, int e, int y, floa
   return true;
 }
 
+// The engine skips rows and windows of a pruned second sweep, not pairs: its pass B rows read
+// every template of the batch.
+template <int EPI>
+__device__ __forceinline__ SkipMask engine_mask(const SkipMask& sk) {
+  SkipMask m{};
+  if constexpr (EPI == EPI_CHUNK) {
+    m.rows = sk.rows;
+    m.windows = sk.windows;
+  }
+  return m;
+}
+
 template <typename SPEC, int EPI>
 __global__ void __launch_bounds__(kThreads, 2) pair_engine_kernel(EngineArgs g) {
   extern __shared__ __align__(128) float2 dsm[];  // pass-A tile [NC * L], then pass-B stages [warp][2][NZ]
@@ -237,7 +259,7 @@ __global__ void __launch_bounds__(kThreads, 2) pair_engine_kernel(EngineArgs g) 
         if (it >= nitems) break;
         pass_a_body<kL, SPEC>(tile, g.I, static_cast<const typename SPEC::T*>(g.T), g.A.Q, g.A.b0, g.A.n0, g.A.d,
                               g.twL, it / kGroups, it % kGroups, g.chained != 0,
-                              EPI == EPI_CHUNK ? g.b.alive : nullptr, EPI == EPI_CHUNK ? g.b.alive_win : nullptr);
+                              engine_mask<EPI>(g.b.skip));
       }
     } else if ((phase == 0) != (role == 0) && g.B.valid) {
       // pass B rows: (window, row) of batch B, one warp per row

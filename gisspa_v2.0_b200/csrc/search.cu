@@ -161,12 +161,16 @@ __global__ void peak_flip_kernel(const unsigned long long* __restrict__ in, long
 // whose pixels all have a best z below the threshold holds no chunk pick for any template or
 // angle: the chunk maximum that reaches the threshold lies on a pixel whose best z does.  The
 // margin covers the rounding difference between this z (from the normalised best correlation)
-// and pass B's (from the raw transform).  One warp per row; alive[w][y] by row y of Q (output
-// row (y + l/2) mod l), alive_win[w] set when any row of window w is alive, *count += rows.
+// and pass B's (from the raw transform, possibly of another column-transform shape).  One warp
+// per row; alive[w][y] by row y of Q (output row (y + l/2) mod l), alive_win[w] set when any row
+// of window w is alive, *count += rows.  creq[w] (a float key, min-reduced) is the smallest
+// correlation that reaches the threshold less the margin at any live pixel of the window: a
+// pair whose maximum over the window stays below it holds no pick either.
 constexpr float kAliveMargin = 1e-3f;
 __global__ void row_alive_kernel(const unsigned long long* __restrict__ peak, const float2* __restrict__ ms, int l,
                                  long long rows, float thresh, unsigned char* __restrict__ alive,
-                                 unsigned char* __restrict__ alive_win, unsigned* __restrict__ count) {
+                                 unsigned char* __restrict__ alive_win, unsigned* __restrict__ count,
+                                 unsigned* __restrict__ creq) {
   const long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (row >= rows) return;  // whole warps
@@ -174,21 +178,45 @@ __global__ void row_alive_kernel(const unsigned long long* __restrict__ peak, co
   const int y = (int)(row % l), oy = (y + l / 2) % l;
   const size_t base = ((size_t)w * l + oy) * l;
   bool hit = false;
+  unsigned req = 0xFFFFFFFFu;  // float_key of +inf and above: no bar yet
+  const double t = (double)thresh - (double)kAliveMargin;
   for (int x = lane; x < l; x += 32) {
     const unsigned long long pk = peak[base + x];
     if (!pk) continue;
     const float2 m = ms[base + x];
     const float z = (key_float((uint32_t)(pk >> 32)) - m.x) * m.y;
-    hit = hit || z >= thresh - kAliveMargin;
+    if (z >= thresh - kAliveMargin) {
+      hit = true;
+      // c reaches z = t where c = mu + t / (1 / sigma), rounded down; with 1 / sigma = 0 every c
+      // gives z = 0, which reaches t here
+      const float c = m.y > 0.f ? __double2float_rd((double)m.x + t / (double)m.y) : -INFINITY;
+      req = min(req, float_key(c));
+    }
   }
   hit = __any_sync(0xffffffffu, hit);
+  req = __reduce_min_sync(0xffffffffu, req);
   if (lane == 0) {
     alive[row] = hit ? 1 : 0;
     if (hit) {
       alive_win[w] = 1;
       atomicAdd(count, 1u);
+      atomicMin(creq + w, req);
     }
   }
+}
+
+// Pairs that sweep 2 must transform: those whose maximum correlation over the window (recorded
+// by sweep 1) reaches the window's bar; alive by pair_index, *count += pairs.
+__global__ void pair_alive_kernel(const unsigned* __restrict__ pair_max, const unsigned* __restrict__ creq,
+                                  int n_windows, int n_angles, long long n, unsigned char* __restrict__ alive,
+                                  unsigned* __restrict__ count) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned pm = pair_max[i];
+  const bool live = pm != 0 && pm >= creq[(i / n_angles) % n_windows];
+  alive[i] = live ? 1 : 0;
+  const unsigned b = __ballot_sync(__activemask(), live);
+  if (b && (threadIdx.x & 31) == __ffs(b) - 1) atomicAdd(count, (unsigned)__popc(b));
 }
 
 // Top-K: image map of the max z over windows covering each pixel (ties: lowest window).
@@ -333,20 +361,47 @@ void window_spectra(Ctx& c, const float* img, int nx, int ny, const std::vector<
 
 // RotateTemplate (norm.cu:479-521): rotate, mask, (x - mean)/sqrt(var), FFT / l^2.
 // st (optional): take the angle from device memory (graph replays); theta is then unused.
-void template_spectra_at(Ctx& c, float theta, const AngleState* st = nullptr) {
+// Rotation by theta, forward transform and scaling of n prepared templates (src) into spectra
+// (dst, in the storage type of the search's precision).
+void spectra_of(Ctx& c, float theta, const float* src, int n, void* dst, const AngleState* st) {
   gisspa_handle* h = c.h;
   const int l = c.l, nt = h->nt, hs = l / 2 + 1;
   const double rad = (double)theta * kRefPi / 180.0;
   float2* rot = buf<float2>(h->rot, (size_t)nt * c.L2);
   float2* rtmp = buf<float2>(h->rot_tmp, (size_t)nt * hs * l);
   double* sums = buf<double>(h->rsums, 2 * (size_t)nt);
-  rotate_batch(h->prep_real.as<float>(), nt, l, (float)std::cos(rad), (float)std::sin(rad), true, h->cfg.diameter,
-               h->cfg.edge_half_width, rot, sums, c.s, st);
-  h->fft.rows(rot, (long long)nt * l, l, -1, 1.f, c.s);
-  h->fft.transpose(rot, rtmp, nt, l, l, c.s, hs);
-  h->fft.rows(rtmp, (long long)nt * hs, l, -1, 1.f, c.s);
+  rotate_batch(src, n, l, (float)std::cos(rad), (float)std::sin(rad), true, h->cfg.diameter, h->cfg.edge_half_width,
+               rot, sums, c.s, st);
+  h->fft.rows(rot, (long long)n * l, l, -1, 1.f, c.s);
+  h->fft.transpose(rot, rtmp, n, l, l, c.s, hs);
+  h->fft.rows(rtmp, (long long)n * hs, l, -1, 1.f, c.s);
+  finalize_spectra(rtmp, n, l, sums, h->cfg.spectrum_precision, dst, 1.0 / (double)c.L2, c.s);
+}
+
+void template_spectra_at(Ctx& c, float theta, const AngleState* st = nullptr) {
+  gisspa_handle* h = c.h;
+  const int l = c.l, nt = h->nt, hs = l / 2 + 1;
   void* ts = h->tspec.ensure(spec_bytes(h->cfg.spectrum_precision) * (size_t)nt * hs * l);
-  finalize_spectra(rtmp, nt, l, sums, h->cfg.spectrum_precision, ts, 1.0 / (double)c.L2, c.s);
+  spectra_of(c, theta, h->prep_real.as<float>(), nt, ts, st);
+}
+
+// The spectra of the listed templates only, in their places among the template spectra (the
+// others keep what an earlier angle left there: the pruned second sweep reads none of them).
+// Each template's transform is independent of the others': the same values as for all.
+void template_spectra_listed(Ctx& c, float theta, const std::vector<int>& list) {
+  gisspa_handle* h = c.h;
+  const int l = c.l, nt = h->nt, hs = l / 2 + 1, n = (int)list.size();
+  const size_t tb = spec_bytes(h->cfg.spectrum_precision) * (size_t)hs * l;
+  float* sub = buf<float>(h->prep_sub, (size_t)nt * c.L2);  // sized for all: allocated once
+  char* ts_sub = static_cast<char*>(h->tspec_sub.ensure(tb * nt));
+  char* ts = static_cast<char*>(h->tspec.ensure(tb * nt));
+  const float* src = h->prep_real.as<float>();
+  for (int i = 0; i < n; ++i)
+    GISSPA_CUDA(cudaMemcpyAsync(sub + (size_t)i * c.L2, src + (size_t)list[i] * c.L2, sizeof(float) * c.L2,
+                                cudaMemcpyDeviceToDevice, c.s));
+  spectra_of(c, theta, sub, n, ts_sub, nullptr);
+  for (int i = 0; i < n; ++i)
+    GISSPA_CUDA(cudaMemcpyAsync(ts + (size_t)list[i] * tb, ts_sub + (size_t)i * tb, tb, cudaMemcpyDeviceToDevice, c.s));
 }
 
 void choose_batches(const gisspa_config& cfg, int l, int W, int nt, int& D, int& E) {
@@ -419,6 +474,15 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
                     : l == 320  ? std::size(c320)
                                 : std::size(c256);
   std::vector<Cand> cands(cb, cb + nc);
+  if (epi == EPI_CHUNK && args.skip.pairs) {
+    // a pruned second sweep transforms a few pairs per angle: its launches are mostly CTAs that
+    // leave at once, so larger batches (up to 1 GiB of Q) take fewer launches
+    const long long per_pair = (long long)(l / 2) * l * (long long)sizeof(float2);
+    cands.clear();
+    for (int dd : {kMaxListedTemplates, 64})
+      for (int ee : {64, 16})
+        if ((long long)dd * ee * per_pair <= (1LL << 30)) cands.push_back(Cand{dd, ee});
+  }
   int maxE = 1, maxDE = 1;
   for (auto& cd : cands) {
     cd.D = std::max(1, std::min(cd.D, nt));
@@ -438,10 +502,11 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
   args.cand_count = reinterpret_cast<unsigned*>(args.nn_sum + 2 * nn);
   args.cand_cap = 0;
   args.cand = nullptr;
+  args.pair_max = nullptr;
   args.nt_total = nt;
   args.err = h->dev_err.as<unsigned>();
-  // (twice the largest batch: the pair engine alternates two Q slots)
-  float2* Q = buf<float2>(h->Q, 2 * (size_t)maxDE * (l / 2) * l);
+  // (twice the largest batch when the pair engine, which alternates two Q slots, is tuned)
+  float2* Q = buf<float2>(h->Q, (kTuneEngine ? 2 : 1) * (size_t)maxDE * (l / 2) * l);
   args.Q = Q;
   const float2* twL = h->fft.twiddles(l);
   const float2* twNZ = h->fft.twiddles(l / 2);
@@ -470,7 +535,9 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
         continue;
       }
       if (!correlate_variant_ok(l, v, epi)) continue;
-      for (int av = 0; av < pass_a_variants(l); ++av) {
+      // (a pruned second sweep's few live pairs do not need the column shape tuned)
+      const int n_av = (epi == EPI_CHUNK && args.skip.pairs) ? 1 : pass_a_variants(l);
+      for (int av = 0; av < n_av; ++av) {
         CorrLaunch cl{l, cd.E, cd.D, h->cfg.spectrum_precision, epi, v};
         cl.tc = h->cfg.tensor_cores != 0;
         cl.a_variant = av;
@@ -591,7 +658,7 @@ long long correlate_all(Ctx& c, int epi, const float2* I, int W, const void* T, 
     h->seq_launches[seq] = launches;
     h->seq_pairs[seq] = pairs;
     h->seq_d[seq] = dsum;
-    h->seq_pruned[seq] = epi == EPI_CHUNK && args.alive != nullptr;
+    h->seq_pruned[seq] = epi == EPI_CHUNK && args.skip.rows != nullptr;
   }
   return pairs;
 }
@@ -700,7 +767,8 @@ std::vector<unsigned char> angle_graph_key(Ctx& c, const NormRun& r, int epi) {
                         (const void*)h->tspec.as<void>(), (const void*)h->ispec.as<void>(),
                         (const void*)h->Q.as<void>(), (const void*)h->gen_z.as<void>(),
                         (const void*)h->gen_x.as<void>(), (const void*)a.S1, (const void*)a.S2, (const void*)a.peak,
-                        (const void*)a.musig, (const void*)a.alive, (const void*)a.alive_win,
+                        (const void*)a.musig, (const void*)a.skip.rows, (const void*)a.skip.windows,
+                        (const void*)a.skip.pairs, (const void*)a.pair_max,
                         (const void*)a.offx, (const void*)a.offy,
                         (const void*)a.cand, (const void*)a.cand_count, (const void*)h->dev_err.as<void>(),
                         (const void*)h->angle_table.as<void>(), (const void*)h->angle_cursor.as<void>(),
@@ -817,18 +885,61 @@ void norm_stats(Ctx& c, NormRun& r) {
   GISSPA_LAUNCH_CHECK();
   r.args.musig = ms;
   if (r.prune) {
-    const long long rows = (long long)r.W * c.l;
-    unsigned char* alive = buf<unsigned char>(c.h->alive, (size_t)rows + r.W);
-    unsigned* cnt = buf<unsigned>(c.h->alive_count, 1);
+    gisspa_handle* h = c.h;
+    const long long rows = (long long)r.W * c.l, npairs = (long long)r.W * r.n_angles * h->nt;
+    unsigned char* alive = buf<unsigned char>(h->alive, (size_t)rows + r.W + npairs);
+    unsigned* cnt = buf<unsigned>(h->alive_count, 2 + r.W);  // rows, pairs, per-window bars
     GISSPA_CUDA(cudaMemsetAsync(alive + rows, 0, r.W, c.s));
-    GISSPA_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned), c.s));
+    GISSPA_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), c.s));
+    GISSPA_CUDA(cudaMemsetAsync(cnt + 2, 0xFF, sizeof(unsigned) * r.W, c.s));
     row_alive_kernel<<<ceil_div(rows * 32, 256), 256, 0, c.s>>>(r.args.peak, ms, c.l, rows, r.args.thresh, alive,
-                                                               alive + rows, cnt);
+                                                               alive + rows, cnt, cnt + 2);
     GISSPA_LAUNCH_CHECK();
-    r.args.alive = alive;
-    r.args.alive_win = alive + rows;
+    pair_alive_kernel<<<ceil_div(npairs, 256), 256, 0, c.s>>>(r.args.pair_max, cnt + 2, r.W, r.n_angles, npairs,
+                                                              alive + rows + r.W, cnt + 1);
+    GISSPA_LAUNCH_CHECK();
+    SkipMask& sk = r.args.skip;
+    sk.rows = alive;
+    sk.windows = alive + rows;
+    sk.pairs = alive + rows + r.W;
+    sk.nt_total = h->nt;
+    sk.n_windows = r.W;
+    sk.n_angles = r.n_angles;
   }
   r.phase = 3;
+}
+
+// A pruned second sweep over angles [a0, a1): from the host copy of the live pairs, each angle
+// with any transforms the spectra of its live templates only and correlates (the launches skip
+// the dead pairs); angles without a live pair are skipped.  Launched from the host (the
+// templates differ from angle to angle).
+void pruned_angles(Ctx& c, NormRun& r, int a0, int a1) {
+  gisspa_handle* h = c.h;
+  const int nt = h->nt, W = r.W, A = r.n_angles;
+  if (r.live_templates.empty()) {
+    std::vector<unsigned char> pa((size_t)W * A * nt);
+    GISSPA_CUDA(cudaMemcpyAsync(pa.data(), r.args.skip.pairs, pa.size(), cudaMemcpyDeviceToHost, c.s));
+    GISSPA_CUDA(cudaStreamSynchronize(c.s));
+    r.live_templates.assign(A, {});
+    for (int t = 0; t < nt; ++t)
+      for (int a = 0; a < A; ++a)
+        for (int w = 0; w < W; ++w)
+          if (pa[pair_index(w, t, a, W, A)]) {
+            r.live_templates[a].push_back(t);
+            break;
+          }
+  }
+  for (int a = a0; a < a1; ++a) {
+    const std::vector<int>& list = r.live_templates[a];
+    if (list.empty()) {
+      r.pairs += (long long)W * nt;  // searched: every pair of this angle is known to hold no pick
+      continue;
+    }
+    template_spectra_listed(c, r.angles[a], list);
+    r.args.angle = a;
+    r.args.angle_state = nullptr;
+    r.pairs += correlate_all(c, EPI_CHUNK, h->ispec.as<float2>(), W, h->tspec.as<void>(), nt, r.args, r.D, r.E);
+  }
 }
 
 // Sweep 2 (PickParticles norm.cu:554-600) over angles [a0, a1): chunk candidates, grown and
@@ -845,16 +956,21 @@ void norm_sweep2(Ctx& c, NormRun& r, int a0, int a1) {
     r.args.cand = cand;
     r.args.cand_count = cnt;
     r.args.cand_cap = cap;
-    run_angles(c, r, EPI_CHUNK, a0, a1);
+    if (r.args.skip.pairs)
+      pruned_angles(c, r, a0, a1);
+    else
+      run_angles(c, r, EPI_CHUNK, a0, a1);
     GISSPA_CUDA(cudaEventRecord(h->ev[3], c.s));
-    unsigned count = 0, alive_rows = 0;
+    unsigned count = 0, alive_n[2] = {0, 0};
     GISSPA_CUDA(cudaMemcpyAsync(&count, cnt, sizeof(unsigned), cudaMemcpyDeviceToHost, c.s));
-    if (r.args.alive)
-      GISSPA_CUDA(cudaMemcpyAsync(&alive_rows, h->alive_count.as<unsigned>(), sizeof(unsigned),
+    if (r.args.skip.rows)
+      GISSPA_CUDA(cudaMemcpyAsync(alive_n, h->alive_count.as<unsigned>(), 2 * sizeof(unsigned),
                                   cudaMemcpyDeviceToHost, c.s));
     GISSPA_CUDA(cudaStreamSynchronize(c.s));
     h->st.candidates = count;
-    h->st.rows_alive = r.args.alive ? (double)alive_rows / ((double)r.W * c.l) : 1.0;
+    h->st.rows_alive = r.args.skip.rows ? (double)alive_n[0] / ((double)r.W * c.l) : 1.0;
+    h->st.pairs_alive =
+        r.args.skip.pairs ? (double)alive_n[1] / ((double)r.W * r.n_angles * h->nt) : 1.0;
     if (count > cap) {  // grow and repeat the second sweep only
       cap = count + count / 4 + 1024;
       continue;
@@ -967,9 +1083,15 @@ void search_norm(Ctx& c, const float* d_img, int nx, int ny, std::vector<gisspa_
   NormRun& r = h->run;
   norm_prepare(c, d_img, nx, ny, r);
   r.prune = h->cfg.prune_sweep2 != 0 && !r.topk && correlate_fast(c.l);
-  if (r.prune) {  // sweep 1 keeps each pixel's best correlation
+  if (r.prune) {  // sweep 1 keeps each pixel's best correlation and each pair's maximum
     r.args.peak = buf<unsigned long long>(h->peak, r.npix);
     GISSPA_CUDA(cudaMemsetAsync(r.args.peak, 0, sizeof(unsigned long long) * r.npix, c.s));
+    r.n_angles = (int)r.angles.size();
+    const size_t npairs = (size_t)r.W * r.n_angles * h->nt;
+    r.args.pair_max = buf<unsigned>(h->pair_max, npairs);
+    r.args.n_windows = r.W;
+    r.args.n_angles = r.n_angles;
+    GISSPA_CUDA(cudaMemsetAsync(r.args.pair_max, 0, sizeof(unsigned) * npairs, c.s));
   }
   const int A = (int)r.angles.size();
   norm_sweep1(c, r, 0, A);
@@ -1721,6 +1843,7 @@ int run_batch(gisspa_handle* h, int n, const float* const* images, const int* nx
     total.graph_replays += h->st.graph_replays;
     total.window_size = h->st.window_size;
     total.rows_alive += h->st.rows_alive / n;
+    total.pairs_alive += h->st.pairs_alive / n;
     total.pass_a_variant = h->st.pass_a_variant;
     total.pass_b_variant = h->st.pass_b_variant;
     all.insert(all.end(), one.begin(), one.end());

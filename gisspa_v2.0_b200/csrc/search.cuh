@@ -33,7 +33,9 @@ struct NormRun {
   std::vector<float> angles;
   double Ntot = 0;
   bool topk = false;
-  bool prune = false;  // sweep 2 skips the rows that cannot hold a pick (search_norm only)
+  bool prune = false;  // sweep 2 skips the rows and pairs that cannot hold a pick (search_norm only)
+  int n_angles = 0;
+  std::vector<std::vector<int>> live_templates;  // pruned second sweep: per angle, host copy
   int D = 1, E = 1;
   CorrArgs args{};
   long long pairs = 0;
@@ -81,7 +83,8 @@ struct gisspa_handle {
   gisspa::DevBuf S1, S2, peak, musig;
   // correlation intermediate and outputs
   gisspa::DevBuf Q, cand, cand_count, nn_key, nn_sum, zkey, zcand, zcount;
-  gisspa::DevBuf alive, alive_count;  // rows sweep 2 transforms (prune_sweep2)
+  gisspa::DevBuf alive, alive_count, pair_max;  // rows and pairs sweep 2 transforms (prune_sweep2)
+  gisspa::DevBuf prep_sub, tspec_sub;            // the live templates of an angle of that sweep
   gisspa::DevBuf engine_ctr;  // work counters of the pair engine, one block per launch of a sequence
   gisspa::DevBuf gen_z, gen_x;  // workspace of the generic correlation (window sizes without tuned kernels)
   gisspa::DevBuf dev_err;  // set by kernels whose bounded waits gave up

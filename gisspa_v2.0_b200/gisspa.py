@@ -108,7 +108,7 @@ class Stats(C.Structure):
                 ("pass_samples", C.c_int), ("window_size", C.c_int), ("pass_b_variant", C.c_int),
                 ("tuned_us_per_pair", C.c_double), ("graph_replays", C.c_longlong), ("corr_pair_us", C.c_double),
                 ("corr_timed_launches", C.c_longlong), ("pass_a_variant", C.c_int),
-                ("rows_alive", C.c_double)]
+                ("rows_alive", C.c_double), ("pairs_alive", C.c_double)]
 
 
 class ShardInfo(C.Structure):

@@ -155,6 +155,8 @@ typedef struct gisspa_stats {
   double rows_alive;           /* fraction of window rows sweep 2 transformed (below 1 with
                                   prune_sweep2; 0 when the search has no second sweep; a batch
                                   reports the mean over its micrographs) */
+  double pairs_alive;          /* fraction of (window, template, angle) pairs sweep 2 transformed
+                                  (same conventions) */
 } gisspa_stats;
 
 typedef struct gisspa_handle gisspa_handle;
