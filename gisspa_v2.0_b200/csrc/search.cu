@@ -251,6 +251,17 @@ __global__ void angle_select_kernel(const AngleState* __restrict__ table, int* _
 
 __global__ void set_int_kernel(int* p, int v) { *p = v; }
 
+// Copies of whole per-template blocks (n4 16-byte words each) by a list of template indices:
+// dst[i] = src[list[i]] (gather) or dst[list[i]] = src[i] (scatter).
+template <bool GATHER>
+__global__ void template_copy_kernel(const uint4* __restrict__ src, const int* __restrict__ list, long long n4,
+                                     uint4* __restrict__ dst) {
+  const int i = blockIdx.y;
+  const long long from = GATHER ? list[i] : i, to = GATHER ? i : list[i];
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n4; k += (long long)gridDim.x * blockDim.x)
+    dst[to * n4 + k] = src[from * n4 + k];
+}
+
 // A bounded wait on an mbarrier phase that never completes (its single expected arrival is
 // never made, and no asynchronous copy targets it): the wait gives up after max_cycles and the
 // CTA raises the error flag, exactly as pass B does when its bulk copies do not land.
@@ -391,17 +402,25 @@ void template_spectra_at(Ctx& c, float theta, const AngleState* st = nullptr) {
 void template_spectra_listed(Ctx& c, float theta, const std::vector<int>& list) {
   gisspa_handle* h = c.h;
   const int l = c.l, nt = h->nt, hs = l / 2 + 1, n = (int)list.size();
+  if (2 * n > nt) {  // most templates: transforming all of them costs less than the copies
+    template_spectra_at(c, theta);
+    return;
+  }
   const size_t tb = spec_bytes(h->cfg.spectrum_precision) * (size_t)hs * l;
-  float* sub = buf<float>(h->prep_sub, (size_t)nt * c.L2);  // sized for all: allocated once
-  char* ts_sub = static_cast<char*>(h->tspec_sub.ensure(tb * nt));
+  float* sub = buf<float>(h->prep_sub, (size_t)nt * c.L2 / 2);  // sized for half of them: allocated once
+  char* ts_sub = static_cast<char*>(h->tspec_sub.ensure(tb * (nt / 2)));
   char* ts = static_cast<char*>(h->tspec.ensure(tb * nt));
-  const float* src = h->prep_real.as<float>();
-  for (int i = 0; i < n; ++i)
-    GISSPA_CUDA(cudaMemcpyAsync(sub + (size_t)i * c.L2, src + (size_t)list[i] * c.L2, sizeof(float) * c.L2,
-                                cudaMemcpyDeviceToDevice, c.s));
+  int* dlist = buf<int>(h->list_dev, (size_t)nt);
+  GISSPA_CUDA(cudaMemcpyAsync(dlist, list.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c.s));
+  static_assert(sizeof(float) * 4 == sizeof(uint4), "16-byte words");
+  const long long w_in = (long long)c.L2 / 4, w_out = (long long)(tb / sizeof(uint4));
+  template_copy_kernel<true><<<dim3(64, n), 256, 0, c.s>>>(reinterpret_cast<const uint4*>(h->prep_real.as<float>()),
+                                                          dlist, w_in, reinterpret_cast<uint4*>(sub));
+  GISSPA_LAUNCH_CHECK();
   spectra_of(c, theta, sub, n, ts_sub, nullptr);
-  for (int i = 0; i < n; ++i)
-    GISSPA_CUDA(cudaMemcpyAsync(ts + (size_t)list[i] * tb, ts_sub + (size_t)i * tb, tb, cudaMemcpyDeviceToDevice, c.s));
+  template_copy_kernel<false><<<dim3(64, n), 256, 0, c.s>>>(reinterpret_cast<const uint4*>(ts_sub), dlist, w_out,
+                                                           reinterpret_cast<uint4*>(ts));
+  GISSPA_LAUNCH_CHECK();
 }
 
 void choose_batches(const gisspa_config& cfg, int l, int W, int nt, int& D, int& E) {
@@ -478,10 +497,12 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
     // a pruned second sweep transforms a few pairs per angle: its launches are mostly CTAs that
     // leave at once, so larger batches (up to 1 GiB of Q) take fewer launches
     const long long per_pair = (long long)(l / 2) * l * (long long)sizeof(float2);
+    const long long cap = std::max(1LL, (1LL << 30) / per_pair);  // pairs in 1 GiB: 4096 .. 256
     cands.clear();
-    for (int dd : {kMaxListedTemplates, 64})
-      for (int ee : {64, 16})
-        if ((long long)dd * ee * per_pair <= (1LL << 30)) cands.push_back(Cand{dd, ee});
+    for (int dd : {kMaxListedTemplates, 64, 16})
+      for (int ee : {64, 16, 4})
+        if ((long long)std::min(dd, nt) * std::min(ee, W) <= cap) cands.push_back(Cand{dd, ee});
+    if (cands.empty()) cands.push_back(Cand{16, 4});
   }
   int maxE = 1, maxDE = 1;
   for (auto& cd : cands) {
@@ -935,7 +956,13 @@ void pruned_angles(Ctx& c, NormRun& r, int a0, int a1) {
       r.pairs += (long long)W * nt;  // searched: every pair of this angle is known to hold no pick
       continue;
     }
-    template_spectra_listed(c, r.angles[a], list);
+    // (the pair engine, selectable as a fixed shape, reads every template of its batches)
+    const bool engine = h->cfg.pass_b_shape == engine_variant(c.l) && h->cfg.template_batch > 0 &&
+                        h->cfg.window_batch > 0;
+    if (engine)
+      template_spectra_at(c, r.angles[a]);
+    else
+      template_spectra_listed(c, r.angles[a], list);
     r.args.angle = a;
     r.args.angle_state = nullptr;
     r.pairs += correlate_all(c, EPI_CHUNK, h->ispec.as<float2>(), W, h->tspec.as<void>(), nt, r.args, r.D, r.E);

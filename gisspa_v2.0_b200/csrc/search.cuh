@@ -84,7 +84,7 @@ struct gisspa_handle {
   // correlation intermediate and outputs
   gisspa::DevBuf Q, cand, cand_count, nn_key, nn_sum, zkey, zcand, zcount;
   gisspa::DevBuf alive, alive_count, pair_max;  // rows and pairs sweep 2 transforms (prune_sweep2)
-  gisspa::DevBuf prep_sub, tspec_sub;            // the live templates of an angle of that sweep
+  gisspa::DevBuf prep_sub, tspec_sub, list_dev;  // the live templates of an angle of that sweep
   gisspa::DevBuf engine_ctr;  // work counters of the pair engine, one block per launch of a sequence
   gisspa::DevBuf gen_z, gen_x;  // workspace of the generic correlation (window sizes without tuned kernels)
   gisspa::DevBuf dev_err;  // set by kernels whose bounded waits gave up

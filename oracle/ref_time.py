@@ -74,10 +74,10 @@ def run(binary: str, config: str, cwd: str, timeout: float) -> float:
     return el
 
 
-def time_binaries(wl: str, binaries: dict, timeout: float = 900.0, single: bool = False) -> dict:
+def time_binaries(wl: str, binaries: dict, timeout: float = 900.0, single: bool = False, repeat: int = 1) -> dict:
     """Per-micrograph and set-up wall time of each binary ({name: path}) on the workload's files
     (single: one run on a one-micrograph list, whose time includes the set-up)."""
-    res = {"workload": wl, "params": synth.SEARCH_PARAMS[wl],
+    res = {"workload": wl, "params": synth.SEARCH_PARAMS[wl], "repeat": repeat,
            "timing": ("wall clock of the whole process on one micrograph (set-up included)" if single else
                       "wall clock of the whole process; per_micrograph = t(2 micrographs) - t(1)")}
     with tempfile.TemporaryDirectory() as d:
@@ -88,7 +88,7 @@ def time_binaries(wl: str, binaries: dict, timeout: float = 900.0, single: bool 
                 cfg = os.path.join(d, f"config_{name}_{n}")
                 out = os.path.join(d, f"picks_{name}_{n}.txt")
                 write_config(cfg, wl, d, lst, n, out)
-                t[n] = run(binary, cfg, d, timeout)
+                t[n] = min(run(binary, cfg, d, timeout) for _ in range(max(1, repeat)))
                 if n == 1:
                     with open(out) as fh:
                         res[f"{name}_picks"] = sum(1 for ln in fh if ln.strip())
@@ -109,8 +109,9 @@ def main():
     ap.add_argument("--ours", default=os.path.join(REPO, "gisspa_v2.0_b200", "_build", "gisspa_main"))
     ap.add_argument("--timeout", type=float, default=900.0)
     ap.add_argument("--single", action="store_true", help="one run on one micrograph (set-up included)")
+    ap.add_argument("--repeat", type=int, default=1, help="runs of each list; the fastest counts")
     a = ap.parse_args()
-    print(json.dumps(time_binaries(a.workload, {"reference": a.ref, "ours": a.ours}, a.timeout, a.single)))
+    print(json.dumps(time_binaries(a.workload, {"reference": a.ref, "ours": a.ours}, a.timeout, a.single, a.repeat)))
 
 
 if __name__ == "__main__":
