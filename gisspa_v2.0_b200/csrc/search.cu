@@ -494,15 +494,14 @@ TuneChoice autotune(Ctx& c, int epi, const float2* I, int W, const void* T, int 
                                 : std::size(c256);
   std::vector<Cand> cands(cb, cb + nc);
   if (epi == EPI_CHUNK && args.skip.pairs) {
-    // a pruned second sweep transforms a few pairs per angle: its launches are mostly CTAs that
-    // leave at once, so larger batches (up to 1 GiB of Q) take fewer launches
+    // a pruned second sweep transforms a few pairs per angle and is launched from the host: its
+    // launches are mostly CTAs that leave at once, and the fewer the better, so one batch shape,
+    // the largest within 4 GiB of Q (only the row-transform shape is tuned)
     const long long per_pair = (long long)(l / 2) * l * (long long)sizeof(float2);
-    const long long cap = std::max(1LL, (1LL << 30) / per_pair);  // pairs in 1 GiB: 4096 .. 256
-    cands.clear();
-    for (int dd : {kMaxListedTemplates, 64, 16})
-      for (int ee : {64, 16, 4})
-        if ((long long)std::min(dd, nt) * std::min(ee, W) <= cap) cands.push_back(Cand{dd, ee});
-    if (cands.empty()) cands.push_back(Cand{16, 4});
+    const long long cap = std::max(1LL, (4LL << 30) / per_pair);  // pairs in 4 GiB: 16384 .. 1024
+    const int dd = std::min(nt, kMaxListedTemplates);
+    const int ee = (int)std::max(1LL, std::min<long long>(W, cap / dd));
+    cands.assign(1, Cand{dd, ee});
   }
   int maxE = 1, maxDE = 1;
   for (auto& cd : cands) {
