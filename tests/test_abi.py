@@ -39,6 +39,7 @@ def test_config_defaults_match_reference():
     assert c.edge_half_width == 4.0 and c.ampconst == pytest.approx(0.07) and c.a == pytest.approx(-10.81)
     assert c.quirks == gisspa.QUIRKS_REFERENCE and c.tile_size == 720
     assert c.cuda_graphs == 1 and c.pass_b_shape == -1
+    assert c.pass_a_shape == -1 and c.prune_sweep2 == 1 and c.tensor_cores == 0
 
 
 def test_config_file_parsing(tmp_path):
@@ -48,12 +49,13 @@ def test_config_file_parsing(tmp_path):
                  "output = out.lst\nfirst = 2\nlast = 9\nGPU_ID = 1\nwindow_size = 512\nphase_flip = 1\n"
                  "overlap = 192\nnorm_type = 1\ninvert = 1\nunknown_key = whatever\npick_mode = topk\n"
                  "spectrum_precision = fp16\ntopk = 50\ncuda_graphs = 0\npass_b_shape = 2\ntemplate_batch = 24\n"
-                 "window_batch = 4\n")
+                 "window_batch = 4\npass_a_shape = 1\nprune_sweep2 = 0\n")
     c, r = gisspa.load_config(str(p))
     assert (c.angpix, c.phistep, c.window_size, c.overlap, c.norm_type, c.invert) == (
         pytest.approx(1.3), 5.0, 512, 192, 1, 1)
     assert c.pick_mode == gisspa.PICK_TOPK and c.spectrum_precision == gisspa.SPEC_FP16 and c.topk == 50
     assert (c.cuda_graphs, c.pass_b_shape, c.template_batch, c.window_batch) == (0, 2, 24, 4)
+    assert (c.pass_a_shape, c.prune_sweep2) == (1, 0)
     assert r.input == b"mics.lst" and r.template_path == b"t.hdf" and (r.first, r.last, r.gpu_id) == (2, 9, 1)
 
 
@@ -80,7 +82,7 @@ def test_create_rejects_bad_configs():
     h = C.c_void_p()
     for over in [dict(window_size=300), dict(window_size=16), dict(window_size=4096), dict(phistep=0.0),
                  dict(overlap=600),
-                 dict(pass_b_shape=9), dict(pass_b_shape=-2)]:
+                 dict(pass_b_shape=9), dict(pass_b_shape=-2), dict(pass_a_shape=2), dict(pass_a_shape=-2)]:
         cfg = gisspa.Config.default(angpix=1.0, phistep=5.0, kk=3.0, energy=300.0, cs=2.7, highres=8.0,
                                     lowres=200.0, diameter=100.0, window_size=512, norm_type=1, **{})
         for k, v in over.items():
