@@ -2,6 +2,7 @@
 #include <cmath>
 #include <complex>
 
+#include "fft.cuh"
 #include "fft_smooth.cuh"
 
 namespace gisspa {
@@ -43,6 +44,53 @@ __global__ void fft_pow2_rows_kernel(float2* __restrict__ data, long long nrows,
     __syncthreads();
   }
   for (int i = threadIdx.x; i < total; i += blockDim.x) base[i] = cscale(sm[i], scale);
+}
+
+// Rows of 256, 512 or 1024 points in registers: one warp per row with the correlation kernels'
+// Stockham plans (256 = 8·8·4 and 512 = 16·8·4 with two exchanges, 1024 = 32·32 with one),
+// through the warp's slice of shared memory; the warp's loads and stores of each register's
+// points are coalesced.  Used for the template, window and micrograph transforms of those
+// lengths (per-angle template spectra, §8(a) 9), where the radix-2 kernel above spent a
+// shared-memory round trip and a CTA barrier on each of log2(n) stages.
+template <int N>
+struct RowPlan {
+  static constexpr bool kTwoStage = N == 1024;
+  static constexpr int kRows = N == 1024 ? 4 : 8;  // warps (rows) per CTA: 32 KiB of exchange buffers
+};
+template <int N, int SIGN>
+__global__ void __launch_bounds__(256) fft_reg_rows_kernel(float2* __restrict__ data, long long nrows,
+                                                           const float2* __restrict__ tw, float scale) {
+  constexpr int T = 32, E = N / T, ROWS = RowPlan<N>::kRows;
+  __shared__ __align__(16) float2 sm[ROWS][N];
+  const int w = threadIdx.x / T, tid = threadIdx.x % T;
+  const long long row = (long long)blockIdx.x * ROWS + w;
+  if (row >= nrows) return;  // a whole warp: its exchanges use __syncwarp only
+  float2* p = data + row * N;
+  float2 v[E];
+  if constexpr (RowPlan<N>::kTwoStage) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = p[fft2_in_index<N, T>(tid, e)];
+    fft2s<N, T, SIGN>(v, sm[w], TwGlobal{tw}, tid, [] { __syncwarp(); });
+#pragma unroll
+    for (int e = 0; e < E; ++e) p[fft2_out_index<N, T>(tid, e)] = cscale(v[e], scale);
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = p[fft3_in_index<N, T>(tid, e)];
+    fft3<N, T, SIGN>(v, sm[w], TwGlobal{tw}, tid, [] { __syncwarp(); });
+#pragma unroll
+    for (int e = 0; e < E; ++e) p[fft3_out_index<N, T>(tid, e)] = cscale(v[e], scale);
+  }
+}
+
+template <int N>
+void reg_rows(float2* data, long long nrows, int sign, float scale, const float2* tw, cudaStream_t s) {
+  constexpr int R = RowPlan<N>::kRows;
+  const long long grid = (nrows + R - 1) / R;
+  if (sign < 0)
+    fft_reg_rows_kernel<N, -1><<<(unsigned)grid, 32 * R, 0, s>>>(data, nrows, tw, scale);
+  else
+    fft_reg_rows_kernel<N, 1><<<(unsigned)grid, 32 * R, 0, s>>>(data, nrows, tw, scale);
+  GISSPA_LAUNCH_CHECK();
 }
 
 // One or more rows of a length whose prime factors are 2, 3, 5 and 7 per CTA: load into
@@ -195,6 +243,16 @@ FftEngine::Blue& FftEngine::bluestein(int n) {
 
 void FftEngine::rows(float2* data, long long nrows, int n, int sign, float scale, cudaStream_t s) {
   if (nrows <= 0 || n <= 0) return;
+  if (n == 256 || n == 512 || n == 1024) {
+    const float2* tw = twiddles(n);
+    if (n == 256)
+      reg_rows<256>(data, nrows, sign, scale, tw, s);
+    else if (n == 512)
+      reg_rows<512>(data, nrows, sign, scale, tw, s);
+    else
+      reg_rows<1024>(data, nrows, sign, scale, tw, s);
+    return;
+  }
   if (is_pow2(n)) {
     if (n > 16384) throw CudaError{cudaErrorInvalidValue, "fft length above 16384"};
     int logn = 0;

@@ -1,4 +1,5 @@
-"""The generic FFT engine (radix 2, mixed radix 2/3/4/5/7, Bluestein) against numpy's FFT.
+"""The generic FFT engine (register Stockham rows for 256, 512 and 1024, radix 2, mixed radix
+2/3/4/5/7, Bluestein) against numpy's FFT.
 
 These transforms prepare templates, micrographs and windows (the reference calls cuFFT at
 norm.cu:106-120 and its uses) and, for window sizes without hand-tuned kernels, carry the
@@ -14,7 +15,8 @@ pytestmark = pytest.mark.gpu
 # (length, rows): powers of two, 2/3/5/7-smooth lengths (mixed-radix kernel, incl. the
 # reference's default window 320 and the 5760 edge of a 4092x5760 micrograph), lengths with a
 # prime factor above 7 (Bluestein: 3838 = 2 19 101, 4092 = 4 3 11 31)
-CASES = [(1, 3), (2, 5), (256, 16), (2048, 3), (3, 7), (6, 9), (105, 4), (320, 41), (336, 8), (720, 6),
+CASES = [(1, 3), (2, 5), (256, 16), (256, 13), (512, 21), (1024, 6), (2048, 3), (3, 7), (6, 9), (105, 4),
+         (320, 41), (336, 8), (720, 6),
          (960, 5), (5760, 2), (7168, 1), (53, 6), (176, 5), (3838, 2), (4092, 2)]
 
 
