@@ -46,26 +46,30 @@ __global__ void fft_pow2_rows_kernel(float2* __restrict__ data, long long nrows,
   for (int i = threadIdx.x; i < total; i += blockDim.x) base[i] = cscale(sm[i], scale);
 }
 
-// Rows of 256, 512 or 1024 points in registers: one warp per row with the correlation kernels'
-// Stockham plans (256 = 8·8·4 and 512 = 16·8·4 with two exchanges, 1024 = 32·32 with one),
-// through the warp's slice of shared memory; the warp's loads and stores of each register's
-// points are coalesced.  Used for the template, window and micrograph transforms of those
-// lengths (per-angle template spectra, §8(a) 9), where the radix-2 kernel above spent a
-// shared-memory round trip and a CTA barrier on each of log2(n) stages.
+// Rows of 256, 320, 512 or 1024 points in registers with the correlation kernels' Stockham
+// plans: one warp per row for 256 = 8·8·4 and 512 = 16·8·4 (two exchanges) and 1024 = 32·32 (one),
+// a half warp per row for 320 = 20·4·4, through the team's slice of shared memory; the team's
+// loads and stores of each register's points are coalesced.  Used for the template, window and
+// micrograph transforms of those lengths (per-angle template spectra, §8(a) 9), where the
+// radix-2 and mixed-radix kernels spent a shared-memory round trip and a CTA barrier per stage.
 template <int N>
 struct RowPlan {
   static constexpr bool kTwoStage = N == 1024;
-  static constexpr int kRows = N == 1024 ? 4 : 8;  // warps (rows) per CTA: 32 KiB of exchange buffers
+  static constexpr int kTeam = N == 320 ? 16 : 32;
+  static constexpr int kRows = N == 1024 ? 4 : N == 320 ? 16 : 8;  // rows per CTA: <= 40 KiB of buffers
 };
 template <int N, int SIGN>
 __global__ void __launch_bounds__(256) fft_reg_rows_kernel(float2* __restrict__ data, long long nrows,
                                                            const float2* __restrict__ tw, float scale) {
-  constexpr int T = 32, E = N / T, ROWS = RowPlan<N>::kRows;
+  constexpr int T = RowPlan<N>::kTeam, E = N / T, ROWS = RowPlan<N>::kRows;
   __shared__ __align__(16) float2 sm[ROWS][N];
   const int w = threadIdx.x / T, tid = threadIdx.x % T;
   const long long row = (long long)blockIdx.x * ROWS + w;
-  if (row >= nrows) return;  // a whole warp: its exchanges use __syncwarp only
-  float2* p = data + row * N;
+  // whole warps leave together (their exchanges use __syncwarp); a half-warp team past the
+  // last row transforms zeros beside its partner and stores nothing
+  if ((long long)blockIdx.x * ROWS + (w & ~(32 / T - 1)) >= nrows) return;
+  const bool live = row < nrows;
+  float2* p = data + (live ? row : 0) * N;
   float2 v[E];
   if constexpr (RowPlan<N>::kTwoStage) {
 #pragma unroll
@@ -75,21 +79,22 @@ __global__ void __launch_bounds__(256) fft_reg_rows_kernel(float2* __restrict__ 
     for (int e = 0; e < E; ++e) p[fft2_out_index<N, T>(tid, e)] = cscale(v[e], scale);
   } else {
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = p[fft3_in_index<N, T>(tid, e)];
+    for (int e = 0; e < E; ++e) v[e] = live ? p[fft3_in_index<N, T>(tid, e)] : make_float2(0.f, 0.f);
     fft3<N, T, SIGN>(v, sm[w], TwGlobal{tw}, tid, [] { __syncwarp(); });
+    if (live)
 #pragma unroll
-    for (int e = 0; e < E; ++e) p[fft3_out_index<N, T>(tid, e)] = cscale(v[e], scale);
+      for (int e = 0; e < E; ++e) p[fft3_out_index<N, T>(tid, e)] = cscale(v[e], scale);
   }
 }
 
 template <int N>
 void reg_rows(float2* data, long long nrows, int sign, float scale, const float2* tw, cudaStream_t s) {
-  constexpr int R = RowPlan<N>::kRows;
+  constexpr int R = RowPlan<N>::kRows, T = RowPlan<N>::kTeam;
   const long long grid = (nrows + R - 1) / R;
   if (sign < 0)
-    fft_reg_rows_kernel<N, -1><<<(unsigned)grid, 32 * R, 0, s>>>(data, nrows, tw, scale);
+    fft_reg_rows_kernel<N, -1><<<(unsigned)grid, T * R, 0, s>>>(data, nrows, tw, scale);
   else
-    fft_reg_rows_kernel<N, 1><<<(unsigned)grid, 32 * R, 0, s>>>(data, nrows, tw, scale);
+    fft_reg_rows_kernel<N, 1><<<(unsigned)grid, T * R, 0, s>>>(data, nrows, tw, scale);
   GISSPA_LAUNCH_CHECK();
 }
 
@@ -243,10 +248,12 @@ FftEngine::Blue& FftEngine::bluestein(int n) {
 
 void FftEngine::rows(float2* data, long long nrows, int n, int sign, float scale, cudaStream_t s) {
   if (nrows <= 0 || n <= 0) return;
-  if (n == 256 || n == 512 || n == 1024) {
+  if (n == 256 || n == 320 || n == 512 || n == 1024) {
     const float2* tw = twiddles(n);
     if (n == 256)
       reg_rows<256>(data, nrows, sign, scale, tw, s);
+    else if (n == 320)
+      reg_rows<320>(data, nrows, sign, scale, tw, s);
     else if (n == 512)
       reg_rows<512>(data, nrows, sign, scale, tw, s);
     else
