@@ -239,14 +239,15 @@ __global__ void __launch_bounds__(NW * 32, MINB)
           }
         }
         if constexpr (EPI == EPI_SUMMAX) {
-          // the pair's maximum over the window: this row's, reduced over the team (or warp) and
-          // the CTA's rows in shared memory, and sent once per template (below)
+          // the pair's maximum over the window: this row's, reduced over the warp (the rows of
+          // a warp's teams belong to the same pair) with one integer max on the float keys, then
+          // over the CTA's warps in shared memory, and sent once per template (below)
           if (a.pair_max) {
             float m = -INFINITY;
 #pragma unroll
             for (int i = 0; i < E; ++i) m = fmaxf(m, fmaxf(v[i].x, v[i].y));
-            m = group_max<(TEAM < 32 ? TEAM : 32)>(m);
-            if ((lt & 31) == 0) atomicMax(&pmax_s[k & 1], float_key(m * inv));
+            const unsigned km = __reduce_max_sync(0xffffffffu, float_key(m * inv));
+            if ((threadIdx.x & 31) == 0) atomicMax(&pmax_s[k & 1], km);
           }
         }
       } else if constexpr (EPI == EPI_CHUNK) {
