@@ -50,7 +50,7 @@ __global__ void fft_pow2_rows_kernel(float2* __restrict__ data, long long nrows,
 // plans: one warp per row for 256 = 8·8·4 and 512 = 16·8·4 (two exchanges) and 1024 = 32·32 (one),
 // a half warp per row for 320 = 20·4·4, through the team's slice of shared memory; the team's
 // loads and stores of each register's points are coalesced.  Used for the template, window and
-// micrograph transforms of those lengths (per-angle template spectra, §8(a) 9), where the
+// micrograph transforms of those lengths (the per-angle template spectra above all), where the
 // radix-2 and mixed-radix kernels spent a shared-memory round trip and a CTA barrier per stage.
 template <int N>
 struct RowPlan {
