@@ -955,10 +955,12 @@ void pruned_angles(Ctx& c, NormRun& r, int a0, int a1) {
       r.pairs += (long long)W * nt;  // searched: every pair of this angle is known to hold no pick
       continue;
     }
-    // (the pair engine, selectable as a fixed shape, reads every template of its batches)
-    const bool engine = h->cfg.pass_b_shape == engine_variant(c.l) && h->cfg.template_batch > 0 &&
-                        h->cfg.window_batch > 0;
-    if (engine)
+    // every template's spectra where the launches read dead pairs too: the pair engine (a fixed
+    // shape) and batches of more templates than pass B lists (a fixed template_batch)
+    const bool fixed = h->cfg.template_batch > 0 && h->cfg.window_batch > 0;
+    const bool all = (fixed && h->cfg.pass_b_shape == engine_variant(c.l)) ||
+                     h->cfg.template_batch > kMaxListedTemplates;
+    if (all)
       template_spectra_at(c, r.angles[a]);
     else
       template_spectra_listed(c, r.angles[a], list);

@@ -307,3 +307,18 @@ def test_pruned_second_sweep_gives_the_same_picks(name, raise_threshold):
     assert r0 == 1.0 and 0.0 <= r1 <= 1.0
     if raise_threshold:
         assert r1 < 1.0
+
+
+def test_pruned_second_sweep_with_a_large_template_batch():
+    """A fixed template batch above the 256 templates that pass B lists: the pruned sweep rebuilds
+    every template's spectra at each angle, and the picks equal those without pruning."""
+    img, tmpl, ctf, cfg = small_case("norm_l512_w4")
+    cfg = cfg.copy(threshold=cfg.threshold + 2.0, template_batch=300, window_batch=2, pass_a_shape=0,
+                   pass_b_shape=0)
+    res = []
+    for prune in (0, 1):
+        s = gisspa.Searcher(cfg.copy(prune_sweep2=prune))
+        s.set_templates(tmpl)
+        res.append(s.search(img, ctf))
+        s.close()
+    assert np.array_equal(res[0], res[1])
